@@ -1,0 +1,392 @@
+/*
+ * fpg.h — C ABI of the B200 (sm_100a) backend for the flexpart-gpu
+ * per-particle timestep.
+ *
+ * The reference crate (Improba/flexpart-gpu, Rust + WGSL via wgpu) drives the
+ * step from ForwardTimeLoopDriver::run_timestep (src/simulation/timeloop.rs:915-1316)
+ * through a set of `encode_*_gpu_with_kernel` functions that each append one
+ * compute pass to a wgpu command encoder.  Every function below is the
+ * replacement for one of those seam functions (cited beside it), or for a
+ * buffer owner method it needs.  The conventions:
+ *
+ *  - every call returns fpg_status (int32_t); 0 is success and the negative
+ *    codes mirror the reference's thiserror enums (cited at fpg_status);
+ *  - handles own device memory; callers own every host array they pass;
+ *  - calls are ordered on a CUDA stream: `stream` is a cudaStream_t passed as
+ *    void*, NULL meaning the context's own stream.  A call that returns data
+ *    to the host synchronises that stream first;
+ *  - one context per host thread; a context is bound to one device;
+ *  - no exceptions and no C++ or torch types cross this boundary.
+ *
+ * Particle state lives on the device as structure-of-arrays (one array per
+ * field).  The 96-byte fpg_particle record is only the exchange format of
+ * upload/download, byte-compatible with the reference's #[repr(C)] Particle
+ * (src/particles/mod.rs:76-168).
+ */
+#ifndef FPG_H
+#define FPG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FPG_ABI_VERSION 1
+
+/* src/particles/mod.rs:18 (MAX_SPECIES) and :21 (FLAG_ACTIVE). */
+#define FPG_MAX_SPECIES 4
+#define FPG_FLAG_ACTIVE 1u
+/* Upper bound on vertical wind levels and output heights held on chip.  The
+ * reference caps both at 16 (src/physics/advection.rs:20,
+ * src/gpu/gridding.rs:85); this backend generalises the same scans. */
+#define FPG_MAX_LEVELS 256
+
+typedef int32_t fpg_status;
+enum {
+    FPG_OK = 0,
+    FPG_ERR_INVALID_ARGUMENT = -1,   /* null handle / pointer, bad enum */
+    FPG_ERR_INVALID_TIME_STEP = -2,  /* InvalidTimeStep: gpu/langevin_fused.rs:119, gpu/advection.rs, gpu/deposition.rs */
+    FPG_ERR_ZERO_SHAPE = -3,         /* ZeroShape / ZeroPblShape / ZeroGridShape: gpu/gridding.rs:226, gpu/langevin_fused.rs:122, gpu/pbl.rs:90 */
+    FPG_ERR_VALUE_TOO_LARGE = -4,    /* ValueTooLarge (does not fit u32): gpu/langevin_fused.rs:124 */
+    FPG_ERR_LENGTH_MISMATCH = -5,    /* LengthMismatch: gpu/deposition.rs:328, gpu/wet_deposition.rs:381 */
+    FPG_ERR_INVALID_SPECIES = -6,    /* InvalidSpeciesIndex: gpu/gridding.rs:228 */
+    FPG_ERR_INVALID_MASS_SCALE = -7, /* InvalidMassScale: gpu/gridding.rs:233 */
+    FPG_ERR_INVALID_REFERENCE_HEIGHT = -8, /* InvalidReferenceHeight: gpu/deposition.rs:340 */
+    FPG_ERR_STORE_FULL = -9,         /* ParticleError::StoreFull: particles/mod.rs:516 */
+    FPG_ERR_SHAPE_MISMATCH = -10,    /* ShapeMismatch: gpu/pbl.rs:92 */
+    FPG_ERR_NOT_READY = -11,         /* a required buffer (met bracket, PBL) was never uploaded */
+    FPG_ERR_INVALID_BRACKET = -12,   /* TemporalInterpolationError::InvalidTimeBracket: simulation/timeloop.rs:2093 */
+    FPG_ERR_OUTSIDE_BRACKET = -13,   /* TemporalInterpolationError::TargetOutsideBracket: simulation/timeloop.rs:2104 */
+    FPG_ERR_SIMULATION_COMPLETE = -14, /* TimeLoopError::SimulationComplete: simulation/timeloop.rs:921 */
+    FPG_ERR_INVALID_BOUNDS = -15,    /* ReleaseError::InvalidBounds: release/mod.rs:33 */
+    FPG_ERR_OUT_OF_GRID = -16,       /* ReleaseError::OutOfGridDomain: release/mod.rs:41 */
+    FPG_ERR_TOO_MANY_LEVELS = -17,   /* more than FPG_MAX_LEVELS heights */
+    FPG_ERR_CUDA = -100,             /* any CUDA runtime error (see fpg_last_cuda_error) */
+    FPG_ERR_OUT_OF_MEMORY = -101,
+    FPG_ERR_NO_DEVICE = -102
+};
+
+/* Returns a static string for a status code. */
+const char* fpg_status_string(fpg_status status);
+/* Last CUDA error code (cudaError_t as int) seen by this thread, 0 if none. */
+int32_t fpg_last_cuda_error(void);
+/* FPG_ABI_VERSION of the loaded library. */
+int32_t fpg_abi_version(void);
+
+/* ------------------------------------------------------------------------
+ * Exchange records
+ * ---------------------------------------------------------------------- */
+
+/* One particle, 96 bytes: src/particles/mod.rs:76-168 field for field. */
+typedef struct fpg_particle {
+    float pos_x, pos_y, pos_z;      /* fractional cell offsets, height [m] */
+    int32_t cell_x, cell_y;
+    uint32_t flags;                 /* bit 0 = active */
+    float mass[FPG_MAX_SPECIES];
+    float vel_u, vel_v, vel_w;
+    float turb_u, turb_v, turb_w;
+    int32_t time, timestep, time_mem, time_split;
+    int32_t release_point, class_id, cbt;
+    uint32_t pad0;
+} fpg_particle;
+
+/* Packed surface input of one met cell, 48 bytes: SurfaceCellInputGpu,
+ * src/gpu/pbl.rs:35-50 (cells ordered i*ny + j). */
+typedef struct fpg_surface_cell {
+    float surface_pressure_pa;
+    float temperature_2m_k;
+    float u10_ms, v10_ms;
+    float surface_stress_n_m2;
+    float sensible_heat_flux_w_m2;
+    float solar_radiation_w_m2;
+    float mixing_height_m;           /* <= 0 or non-finite: unavailable */
+    float friction_velocity_ms;      /* <= 0 or non-finite: unavailable */
+    float inv_obukhov_length_per_m;  /* |1/L| < 1e-5 or non-finite: unavailable */
+    float pad0, pad1;
+} fpg_surface_cell;
+
+/* PblComputationOptions, src/io/pbl_params.rs:35-68 (fields the GPU path
+ * reads: src/shaders/pbl_diagnostics.wgsl:46-59). */
+typedef struct fpg_pbl_options {
+    float roughness_length_m;              /* default 0.1 */
+    float wind_reference_height_m;         /* default 10 */
+    float heat_flux_neutral_threshold_w_m2;/* default 1 */
+    float fallback_mixing_height_m;        /* default 800 */
+    float hmix_min_m;                      /* default 100 (lib.rs:44) */
+    float hmix_max_m;                      /* default 4500 (lib.rs:46) */
+} fpg_pbl_options;
+
+/* ------------------------------------------------------------------------
+ * Context
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_ctx fpg_ctx;
+
+/* GpuContext::new (src/gpu/mod.rs:163-208): binds `device`, creates a stream. */
+fpg_status fpg_ctx_create(int32_t device, fpg_ctx** out);
+fpg_status fpg_ctx_destroy(fpg_ctx* ctx);
+/* The context's stream as a cudaStream_t. */
+void* fpg_ctx_stream(fpg_ctx* ctx);
+/* device.poll(Maintain::Wait): waits for all work queued on `stream`. */
+fpg_status fpg_ctx_synchronize(fpg_ctx* ctx, void* stream);
+/* Number of kernels this context has launched since creation (all entry
+ * points, graph replays counted per kernel node). */
+uint64_t fpg_ctx_kernel_launches(fpg_ctx* ctx);
+
+/* ------------------------------------------------------------------------
+ * Particles (ParticleBuffers, src/gpu/buffers.rs:377-510)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_particles fpg_particles;
+
+/* ParticleBuffers::from_store on an empty store: `capacity` zeroed
+ * (inactive) slots; dispatch count = capacity. */
+fpg_status fpg_particles_create(fpg_ctx* ctx, size_t capacity, fpg_particles** out);
+fpg_status fpg_particles_destroy(fpg_particles* p);
+size_t fpg_particles_capacity(const fpg_particles* p);
+/* ParticleBuffers::particle_count / set_dispatch_count / reset_dispatch_count
+ * (buffers.rs:408-436): slots [0, count) are processed by every kernel. */
+size_t fpg_particles_dispatch_count(const fpg_particles* p);
+fpg_status fpg_particles_set_dispatch_count(fpg_particles* p, size_t count);
+/* upload_particle_slots for the contiguous slots [first, first+count)
+ * (buffers.rs:464-492). `records` is host memory. */
+fpg_status fpg_particles_upload(fpg_particles* p, size_t first, size_t count,
+                                const fpg_particle* records, void* stream);
+/* upload_particle_slots for an arbitrary slot list. */
+fpg_status fpg_particles_upload_slots(fpg_particles* p, const uint32_t* slots, size_t count,
+                                     const fpg_particle* records, void* stream);
+/* download_particles (buffers.rs:111-163) for [first, first+count). */
+fpg_status fpg_particles_download(fpg_particles* p, size_t first, size_t count,
+                                  fpg_particle* out, void* stream);
+
+/* Field ids of the structure-of-arrays state, for direct device access. */
+enum {
+    FPG_FIELD_POS_X = 0, FPG_FIELD_POS_Y, FPG_FIELD_POS_Z,
+    FPG_FIELD_CELL_X, FPG_FIELD_CELL_Y, FPG_FIELD_FLAGS,
+    FPG_FIELD_MASS0, FPG_FIELD_MASS1, FPG_FIELD_MASS2, FPG_FIELD_MASS3,
+    FPG_FIELD_VEL_U, FPG_FIELD_VEL_V, FPG_FIELD_VEL_W,
+    FPG_FIELD_TURB_U, FPG_FIELD_TURB_V, FPG_FIELD_TURB_W,
+    FPG_FIELD_TIME, FPG_FIELD_TIMESTEP, FPG_FIELD_TIME_MEM, FPG_FIELD_TIME_SPLIT,
+    FPG_FIELD_RELEASE_POINT, FPG_FIELD_CLASS, FPG_FIELD_CBT,
+    FPG_FIELD_COUNT
+};
+/* Device pointer of one 4-byte-per-slot field array (capacity elements). */
+void* fpg_particles_field(fpg_particles* p, int32_t field);
+/* Copy `count` elements of one field between host and device
+ * (to_device != 0: host -> device).  Host memory may be pinned or pageable. */
+fpg_status fpg_particles_copy_field(fpg_particles* p, int32_t field, size_t first, size_t count,
+                                    void* host, int32_t to_device, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Dual-time wind bracket (DualWindBuffers, src/gpu/buffers.rs:801-950)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_met fpg_met;
+
+fpg_status fpg_met_create(fpg_ctx* ctx, size_t nx, size_t ny, size_t nz, fpg_met** out);
+fpg_status fpg_met_destroy(fpg_met* m);
+/* DualWindBuffers::upload_t0 / upload_t1: `which` 0 = t0, 1 = t1.  u, v, w
+ * are host arrays of nx*ny*nz floats in the reference layout
+ * ((ix*ny)+iy)*nz+iz (z fastest, buffers.rs:229-235). */
+fpg_status fpg_met_upload_frame(fpg_met* m, int32_t which, const float* u, const float* v,
+                                const float* w, void* stream);
+/* Same from device arrays (already resident frames, e.g. a frame ring). */
+fpg_status fpg_met_upload_frame_device(fpg_met* m, int32_t which, const float* u_dev,
+                                       const float* v_dev, const float* w_dev, void* stream);
+/* VelocityToGridScale::level_heights_m (advection.rs:31-41): heights [m] of
+ * the nz wind levels.  All-zero (top <= 0) selects the legacy mode where
+ * pos_z is a level index.  n must equal nz (n <= FPG_MAX_LEVELS). */
+fpg_status fpg_met_set_level_heights(fpg_met* m, const float* heights, size_t n);
+
+/* ------------------------------------------------------------------------
+ * PBL fields (PblBuffers, src/gpu/buffers.rs:955-1060) and per-cell surface
+ * input (SurfaceFieldBuffer, src/gpu/pbl.rs:142-240)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_pbl fpg_pbl;
+typedef struct fpg_surface fpg_surface;
+
+fpg_status fpg_pbl_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_pbl** out);
+fpg_status fpg_pbl_destroy(fpg_pbl* pbl);
+/* PblBuffers::upload_state: host arrays of nx*ny floats (i*ny + j). */
+fpg_status fpg_pbl_upload(fpg_pbl* pbl, const float* ustar, const float* wstar, const float* hmix,
+                          const float* oli, const float* sshf, const float* ssr,
+                          const float* surfstr, void* stream);
+/* Reads the seven PBL fields back (any pointer may be NULL). */
+fpg_status fpg_pbl_download(fpg_pbl* pbl, float* ustar, float* wstar, float* hmix, float* oli,
+                            float* sshf, float* ssr, float* surfstr, void* stream);
+
+fpg_status fpg_surface_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_surface** out);
+fpg_status fpg_surface_destroy(fpg_surface* s);
+/* SurfaceFieldBuffer::upload of one frame: `which` 0 = t0, 1 = t1.  The
+ * device lerps the two frames (io/temporal.rs:122,417-420) inside
+ * fpg_pbl_diagnostics, so a bracket is uploaded once, not every step. */
+fpg_status fpg_surface_upload(fpg_surface* s, int32_t which, const fpg_surface_cell* cells,
+                              void* stream);
+
+/* encode_pbl_diagnostics_gpu_with_kernel (src/gpu/pbl.rs:367) preceded by
+ * interpolate_surface_fields_linear (src/io/temporal.rs:122): per met cell,
+ * lerp the t0/t1 surface frames by `alpha` (0 uses t0 only, 1 t1 only, as the
+ * reference's early returns do), then compute u*, w*, hmix, 1/L into `pbl`.
+ * Errors: ZeroShape, ShapeMismatch. */
+fpg_status fpg_pbl_diagnostics(fpg_ctx* ctx, const fpg_surface* surface, float alpha,
+                               const fpg_pbl_options* options, fpg_pbl* pbl, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Per-cell deposition forcing (2-D, i*ny + j)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_cellfield fpg_cellfield;
+fpg_status fpg_cellfield_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_cellfield** out);
+fpg_status fpg_cellfield_destroy(fpg_cellfield* f);
+/* Uploads per-cell (lambda [1/s], precipitating fraction [-]) pairs. */
+fpg_status fpg_cellfield_upload(fpg_cellfield* f, const float* lambda, const float* fraction,
+                                void* stream);
+/* Derives the per-cell wet forcing from precipitation on the device:
+ * wet_precipitation_state (src/physics/wet_scavenging.rs:179-207) gives the
+ * precipitating fraction and sub-grid rate, then the below-cloud gas
+ * coefficient a * prec^b (wet_scavenging.rs:213-225).  Inputs are host
+ * arrays of large-scale and convective precipitation [mm/h] and cloud cover
+ * [-] (any may be NULL = 0, cloud cover NULL = 1). */
+fpg_status fpg_cellfield_from_precipitation(fpg_cellfield* f, const float* lsp_mm_h,
+                                            const float* convp_mm_h, const float* cloud_cover,
+                                            float gas_coefficient_a, float gas_exponent_b,
+                                            void* stream);
+
+/* ------------------------------------------------------------------------
+ * The fused step
+ * ---------------------------------------------------------------------- */
+enum { /* how a deposition input is supplied */
+    FPG_FORCING_NONE = 0,         /* process skipped (ParticleForcingField::Uniform(0)) */
+    FPG_FORCING_UNIFORM = 1,      /* one scalar for all slots */
+    FPG_FORCING_PER_PARTICLE = 2, /* device arrays indexed by slot (the reference seam) */
+    FPG_FORCING_PER_CELL = 3      /* fpg_cellfield looked up at the particle's nearest cell */
+};
+
+enum { /* stages of fpg_step (bit mask) */
+    FPG_STAGE_ADVECT = 1u,     /* advection_dual_wind.wgsl */
+    FPG_STAGE_TURBULENCE = 2u, /* langevin_fused.wgsl */
+    FPG_STAGE_DRY = 4u,        /* dry_deposition.wgsl */
+    FPG_STAGE_WET = 8u,        /* wet_deposition.wgsl */
+    FPG_STAGE_ALL = 15u
+};
+
+typedef struct fpg_step_params {
+    uint32_t stages;            /* FPG_STAGE_* mask */
+    float alpha;                /* temporal weight of t1; clamped to [0,1] (gpu/advection.rs:639) */
+    float dt_seconds;           /* advection dt (may be negative: backward mode) */
+    float turb_dt_seconds;      /* Langevin / deposition dt (> 0 for turbulence) */
+    float x_grid_per_meter;     /* VelocityToGridScale (physics/advection.rs:36-41) */
+    float y_grid_per_meter;
+    float z_grid_per_meter;
+    uint32_t n_substeps;        /* LangevinStep::n_substeps (physics/langevin.rs:46), 4 in production */
+    float min_height_m;         /* LangevinStep::min_height_m, 0.01 in production */
+    float rho_grad_over_rho;    /* ForwardStepForcing::rho_grad_over_rho */
+    uint32_t key[2];            /* Philox key */
+    uint32_t counter[4];        /* Philox base counter of this step */
+    float dry_reference_height_m; /* DryDepositionStepParams::reference_height_m (15 m) */
+    int32_t dry_mode;           /* FPG_FORCING_* */
+    float dry_velocity_m_s;     /* UNIFORM value */
+    const float* dry_velocity_dev;   /* PER_PARTICLE device array (capacity) */
+    float* dry_probability_dev;      /* optional device output (capacity), NULL = not written */
+    int32_t wet_mode;           /* FPG_FORCING_* */
+    float wet_lambda_s_inv;     /* UNIFORM values */
+    float wet_fraction;
+    const float* wet_lambda_dev;     /* PER_PARTICLE device arrays */
+    const float* wet_fraction_dev;
+    const fpg_cellfield* wet_cells;  /* PER_CELL */
+    float* wet_probability_dev;      /* optional device output (capacity) */
+} fpg_step_params;
+
+/* Fills `params` with the production defaults of the forward loop
+ * (simulation/timeloop.rs:1062-1113): all stages, alpha 0, n_substeps 4,
+ * min height 0.01 m, href 15 m, no deposition forcing, scales 1. */
+void fpg_step_params_default(fpg_step_params* params);
+
+/* One fused pass over slots [0, dispatch_count) of `particles`, replacing, in
+ * this order:
+ *   encode_advection_dual_wind_gpu_with_kernel (src/gpu/advection.rs:605),
+ *   encode_langevin_fused_gpu                  (src/gpu/langevin_fused.rs:133),
+ *   encode_dry_deposition_probability_gpu_with_kernel (src/gpu/deposition.rs:315),
+ *   encode_wet_deposition_probability_gpu_with_kernel (src/gpu/wet_deposition.rs:368).
+ * Each particle is read once and written once.  `next_counter` receives the
+ * Philox counter for the next step (langevin_fused.rs:229-233; unchanged when
+ * the dispatch count is 0 or turbulence is off).  `met` may be NULL when
+ * advection is off, `pbl` when turbulence is off.
+ * Errors: InvalidTimeStep (non-finite dt; turbulence dt <= 0), ZeroShape,
+ * ValueTooLarge, InvalidReferenceHeight, NotReady. */
+fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met,
+                    const fpg_pbl* pbl, const fpg_step_params* params,
+                    uint32_t next_counter[4], void* stream);
+
+/* The four seam functions one at a time (same kernel, one stage). */
+fpg_status fpg_advect_dual_wind(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met,
+                                float alpha, float dt_seconds, float x_grid_per_meter,
+                                float y_grid_per_meter, float z_grid_per_meter, void* stream);
+fpg_status fpg_langevin_fused(fpg_ctx* ctx, fpg_particles* particles, const fpg_pbl* pbl,
+                              float dt_seconds, float rho_grad_over_rho, uint32_t n_substeps,
+                              float min_height_m, const uint32_t key[2],
+                              const uint32_t base_counter[4], uint32_t next_counter[4],
+                              void* stream);
+/* vdep_dev / prob_dev are device arrays of dispatch_count floats (prob may be NULL). */
+fpg_status fpg_dry_deposition(fpg_ctx* ctx, fpg_particles* particles, const float* vdep_dev,
+                              float dt_seconds, float reference_height_m, float* prob_dev,
+                              void* stream);
+fpg_status fpg_wet_deposition(fpg_ctx* ctx, fpg_particles* particles, const float* lambda_dev,
+                              const float* fraction_dev, float dt_seconds, float* prob_dev,
+                              void* stream);
+
+/* ------------------------------------------------------------------------
+ * Concentration gridding (src/gpu/gridding.rs:255-420)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_grid fpg_grid;
+
+fpg_status fpg_grid_create(fpg_ctx* ctx, size_t nx, size_t ny, size_t nz, fpg_grid** out);
+fpg_status fpg_grid_destroy(fpg_grid* g);
+/* dispatch_concentration_gridding_gpu (gridding.rs:255-406): clears the grid,
+ * then bins active slots [0, dispatch_count) into (clamp(cell_x),
+ * clamp(cell_y), level(pos_z)) adding 1 to the count and
+ * u32(mass*scale + 0.5) to the mass grid (concentration_gridding.wgsl:284-345).
+ * `outheights` has nz entries (or NULL = all zero: floor(pos_z) levels).
+ * Integer sums: the result does not depend on thread order.
+ * Errors: ZeroShape, InvalidSpeciesIndex, InvalidMassScale, ValueTooLarge. */
+fpg_status fpg_grid_accumulate(fpg_ctx* ctx, const fpg_particles* particles, fpg_grid* grid,
+                               uint32_t species_index, float mass_scale,
+                               const float* outheights, size_t n_outheights, void* stream);
+/* download_output (gridding.rs:191-219): counts, raw scaled masses and kg
+ * (= scaled / mass_scale as f32); any pointer may be NULL. */
+fpg_status fpg_grid_download(fpg_grid* g, uint32_t* counts, uint32_t* mass_scaled, float* mass_kg,
+                             void* stream);
+/* Device pointers of the count and scaled-mass grids (nx*ny*nz u32 each). */
+uint32_t* fpg_grid_counts_device(fpg_grid* g);
+uint32_t* fpg_grid_mass_device(fpg_grid* g);
+
+/* ------------------------------------------------------------------------
+ * Active-particle compaction (src/gpu/compaction.rs:447-505)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_compaction fpg_compaction;
+
+fpg_status fpg_compaction_create(fpg_ctx* ctx, size_t capacity, fpg_compaction** out);
+fpg_status fpg_compaction_destroy(fpg_compaction* c);
+/* encode_compaction_with_reorder + download_active_count
+ * (compaction.rs:447-505,290-302): a stable scan of the active bit over all
+ * capacity slots; active slots move, in their original order, to
+ * [0, active_count); every slot >= active_count receives its own previous
+ * contents with the active bit cleared (compaction.wgsl:194-217).  Sets the
+ * dispatch count to active_count (timeloop.rs:1254-1261).  `active_count`
+ * (host, may be NULL) receives the count; `compacted_indices_dev` (optional
+ * device array of capacity u32) receives the original slot of each
+ * compacted position. */
+fpg_status fpg_compact(fpg_ctx* ctx, fpg_particles* particles, fpg_compaction* c,
+                       uint32_t* active_count, uint32_t* compacted_indices_dev, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Philox utility (philox_rng.wgsl:441-464, src/gpu/rng.rs:198)
+ * ---------------------------------------------------------------------- */
+/* out_dev (device, 4*n floats): uniforms of blocks counter+0 .. counter+n-1. */
+fpg_status fpg_philox_uniforms(fpg_ctx* ctx, const uint32_t key[2], const uint32_t counter[4],
+                               size_t n_blocks, float* out_dev, uint32_t* out_raw_dev,
+                               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FPG_H */
