@@ -1,0 +1,102 @@
+// fpg_internal.h — handle layouts and launch helpers shared by the .cu files
+// of libfpg.  Nothing here crosses the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/fpg.h"
+
+namespace fpg {
+
+// Records the CUDA error for fpg_last_cuda_error() and maps it to a status.
+fpg_status cuda_status(cudaError_t e);
+
+#define FPG_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t fpg_e_ = (call);                     \
+        if (fpg_e_ != cudaSuccess) return fpg::cuda_status(fpg_e_); \
+    } while (0)
+
+#define FPG_CHECK_LAUNCH() FPG_CUDA(cudaGetLastError())
+
+}  // namespace fpg
+
+struct fpg_ctx {
+    int32_t device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    std::atomic<uint64_t> launches{0};
+    cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
+    void count(uint64_t n = 1) { launches.fetch_add(n, std::memory_order_relaxed); }
+};
+
+struct fpg_particles {
+    fpg_ctx* ctx = nullptr;
+    size_t capacity = 0;
+    size_t dispatch = 0;
+    void* block = nullptr;                  // one allocation, FPG_FIELD_COUNT arrays
+    void* field[FPG_FIELD_COUNT] = {};
+    // Highest species index + 1 with any non-zero mass ever uploaded.  Slots of
+    // higher species are all zero, and zero * survival stays zero, so kernels
+    // skip them without changing any result.
+    int n_species = 1;
+};
+
+struct fpg_met {
+    fpg_ctx* ctx = nullptr;
+    size_t nx = 0, ny = 0, nz = 0;
+    // Node-major bracket: node n holds float4 (u,v,w,0) of t0 at [2n] and of
+    // t1 at [2n+1]; node n = ((ix*ny)+iy)*nz+iz as in the reference layout.
+    float4* bracket = nullptr;
+    float* staging = nullptr;               // 3*nodes floats for host uploads
+    float* heights_dev = nullptr;           // nz level heights on the device
+    float heights[FPG_MAX_LEVELS] = {};
+    bool heights_set = false;
+    bool monotonic = true;
+    bool uploaded[2] = {false, false};
+};
+
+struct fpg_pbl {
+    fpg_ctx* ctx = nullptr;
+    size_t nx = 0, ny = 0;
+    float* field[7] = {};                   // ustar, wstar, hmix, oli, sshf, ssr, surfstr
+    float4* packed = nullptr;               // (ustar, wstar, hmix, oli) per cell
+    bool ready = false;
+};
+
+struct fpg_surface {
+    fpg_ctx* ctx = nullptr;
+    size_t nx = 0, ny = 0;
+    fpg_surface_cell* frame[2] = {};
+    bool uploaded[2] = {false, false};
+};
+
+struct fpg_cellfield {
+    fpg_ctx* ctx = nullptr;
+    size_t nx = 0, ny = 0;
+    float2* lf = nullptr;                   // (lambda, fraction) per cell
+    float* staging = nullptr;               // 3*cells floats
+    bool ready = false;
+};
+
+struct fpg_grid {
+    fpg_ctx* ctx = nullptr;
+    size_t nx = 0, ny = 0, nz = 0;
+    uint32_t* counts = nullptr;
+    uint32_t* mass = nullptr;
+    float mass_scale = 1.0e6f;
+};
+
+struct fpg_compaction {
+    fpg_ctx* ctx = nullptr;
+    size_t capacity = 0;
+    void* block = nullptr;                  // second structure-of-arrays (swapped in)
+    uint32_t* tile_counts = nullptr;        // per-tile active counts, then offsets
+    uint32_t* active_count_dev = nullptr;
+    uint32_t* active_count_host = nullptr;  // pinned
+    size_t n_tiles = 0;
+};

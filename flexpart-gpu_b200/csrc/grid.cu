@@ -1,0 +1,207 @@
+// grid.cu — concentration gridding (concentration_gridding.wgsl:284-345,
+// host side src/gpu/gridding.rs:255-420).
+//
+// Each active particle adds 1 to its cell's count and u32(mass*scale+0.5) to
+// its cell's scaled mass.  Both grids are u32 sums, so the result is the same
+// whatever order the additions happen in.  A warp first merges the particles
+// that share a cell (one __match-style pass per distinct cell in the warp,
+// __reduce_add_sync of the scaled masses) and issues one pair of atomics per
+// distinct cell instead of one per particle; particles released together
+// stay close together, so a warp usually holds very few distinct cells.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "fpg_internal.h"
+
+namespace fpg {
+
+struct LevelTable { float h[FPG_MAX_LEVELS]; };
+
+struct GridArgs {
+    const int32_t* cell_x; const int32_t* cell_y; const float* pos_z; const uint32_t* flags; const float* mass;
+    uint32_t n, nx, ny, nz;
+    float mass_scale;
+    int meters;  // outheights[nz-1] > 0
+};
+
+// pos_z_to_level (concentration_gridding.wgsl:304-315).
+__device__ __forceinline__ uint32_t level_of(float z, const float* h, uint32_t nz, int meters) {
+    if (meters) {
+        for (uint32_t k = 0; k < nz; ++k)
+            if (z <= h[k]) return k;
+        return nz - 1u;
+    }
+    // u32(clamp(i32(floor(z)), 0, nz-1)); float->int conversion saturates
+    const int iz = (int)floorf(z);
+    return (uint32_t)min(max(iz, 0), (int)nz - 1);
+}
+
+// quantize_mass_to_u32 (concentration_gridding.wgsl:317-326).
+__device__ __forceinline__ uint32_t quantize(float m, float scale) {
+    if (m <= 0.0f) return 0u;
+    const float scaled = m * scale + 0.5f;
+    if (scaled >= 4294967295.0f) return 0xffffffffu;
+    return (uint32_t)scaled;
+}
+
+__device__ __forceinline__ uint32_t cell_of(const GridArgs& a, const float* h, uint32_t p) {
+    const int32_t cx = a.cell_x[p], cy = a.cell_y[p];
+    const uint32_t ix = (uint32_t)min(max(cx, 0), (int)a.nx - 1);
+    const uint32_t iy = (uint32_t)min(max(cy, 0), (int)a.ny - 1);
+    const uint32_t iz = level_of(a.pos_z[p], h, a.nz, a.meters);
+    return (ix * a.ny + iy) * a.nz + iz;
+}
+
+__global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, uint32_t* __restrict__ counts,
+                                                   uint32_t* __restrict__ mass) {
+    __shared__ float s_h[FPG_MAX_LEVELS];
+    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_h[i] = lt.h[i];
+    __syncthreads();
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31u;
+    bool valid = false;
+    uint32_t key = 0xffffffffu, q = 0u;
+    if (p < a.n && (a.flags[p] & 1u)) {
+        valid = true;
+        key = cell_of(a, s_h, p);
+        q = quantize(fmaxf(a.mass[p], 0.0f), a.mass_scale);
+    }
+    // warp-uniform loop over the distinct cells held by this warp
+    unsigned pending = __ballot_sync(0xffffffffu, valid);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        const uint32_t k = __shfl_sync(0xffffffffu, key, src);
+        const bool mine = valid && key == k;
+        const unsigned grp = __ballot_sync(0xffffffffu, mine);
+        const uint32_t qs = __reduce_add_sync(0xffffffffu, mine ? q : 0u);
+        if (lane == (unsigned)src) {
+            atomicAdd(counts + k, (uint32_t)__popc(grp));
+            atomicAdd(mass + k, qs);
+        }
+        pending &= ~grp;
+    }
+}
+
+__global__ void __launch_bounds__(256) cell_index_kernel(GridArgs a, LevelTable lt, uint32_t* __restrict__ out) {
+    __shared__ float s_h[FPG_MAX_LEVELS];
+    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_h[i] = lt.h[i];
+    __syncthreads();
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    out[p] = (a.flags[p] & 1u) ? cell_of(a, s_h, p) : 0xffffffffu;
+}
+
+static fpg_status prepare(const fpg_particles* P, const fpg_grid* g, uint32_t species, float scale,
+                          const float* oh, size_t n_oh, GridArgs& a, LevelTable& lt) {
+    if (g->nx == 0 || g->ny == 0 || g->nz == 0) return FPG_ERR_ZERO_SHAPE;
+    if (species >= FPG_MAX_SPECIES) return FPG_ERR_INVALID_SPECIES;            // gridding.rs:262
+    if (!std::isfinite(scale) || scale <= 0.0f) return FPG_ERR_INVALID_MASS_SCALE;  // gridding.rs:268
+    if (oh && n_oh != g->nz) return FPG_ERR_LENGTH_MISMATCH;
+    if (P->dispatch > (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    std::memset(&lt, 0, sizeof(lt));
+    if (oh) std::memcpy(lt.h, oh, g->nz * sizeof(float));
+    a.cell_x = (const int32_t*)P->field[FPG_FIELD_CELL_X];
+    a.cell_y = (const int32_t*)P->field[FPG_FIELD_CELL_Y];
+    a.pos_z = (const float*)P->field[FPG_FIELD_POS_Z];
+    a.flags = (const uint32_t*)P->field[FPG_FIELD_FLAGS];
+    a.mass = (const float*)P->field[FPG_FIELD_MASS0 + species];
+    a.n = (uint32_t)P->dispatch;
+    a.nx = (uint32_t)g->nx; a.ny = (uint32_t)g->ny; a.nz = (uint32_t)g->nz;
+    a.mass_scale = scale;
+    a.meters = lt.h[g->nz - 1] > 0.0f;
+    return FPG_OK;
+}
+
+}  // namespace fpg
+
+using namespace fpg;
+
+extern "C" fpg_status fpg_grid_create(fpg_ctx* ctx, size_t nx, size_t ny, size_t nz, fpg_grid** out) {
+    if (!ctx || !out) return FPG_ERR_INVALID_ARGUMENT;
+    if (nx == 0 || ny == 0 || nz == 0) return FPG_ERR_ZERO_SHAPE;
+    if (nz > FPG_MAX_LEVELS) return FPG_ERR_TOO_MANY_LEVELS;
+    if (nx * ny * nz >= (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    fpg_grid* g = new fpg_grid();
+    g->ctx = ctx; g->nx = nx; g->ny = ny; g->nz = nz;
+    const size_t cells = nx * ny * nz;
+    cudaError_t e = cudaMalloc(&g->counts, cells * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&g->mass, cells * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->counts, 0, cells * sizeof(uint32_t), ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->mass, 0, cells * sizeof(uint32_t), ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(g->counts); cudaFree(g->mass); delete g;
+        return cuda_status(e);
+    }
+    *out = g;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_grid_destroy(fpg_grid* g) {
+    if (!g) return FPG_OK;
+    cudaFree(g->counts);
+    cudaFree(g->mass);
+    delete g;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_grid_accumulate(fpg_ctx* ctx, const fpg_particles* P, fpg_grid* g, uint32_t species,
+                                          float mass_scale, const float* outheights, size_t n_oh, void* stream) {
+    if (!ctx || !P || !g) return FPG_ERR_INVALID_ARGUMENT;
+    GridArgs a;
+    LevelTable lt;
+    fpg_status st = prepare(P, g, species, mass_scale, outheights, n_oh, a, lt);
+    if (st != FPG_OK) return st;
+    cudaStream_t s = ctx->pick(stream);
+    const size_t cells = g->nx * g->ny * g->nz;
+    FPG_CUDA(cudaMemsetAsync(g->counts, 0, cells * sizeof(uint32_t), s));   // outputs.clear (gridding.rs:282)
+    FPG_CUDA(cudaMemsetAsync(g->mass, 0, cells * sizeof(uint32_t), s));
+    g->mass_scale = mass_scale;
+    if (a.n == 0) return FPG_OK;
+    grid_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(a, lt, g->counts, g->mass);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_grid_cell_indices(fpg_ctx* ctx, const fpg_particles* P, const fpg_grid* g,
+                                            const float* outheights, size_t n_oh, uint32_t* out_dev, void* stream) {
+    if (!ctx || !P || !g || !out_dev) return FPG_ERR_INVALID_ARGUMENT;
+    GridArgs a;
+    LevelTable lt;
+    fpg_status st = prepare(P, g, 0, 1.0f, outheights, n_oh, a, lt);
+    if (st != FPG_OK) return st;
+    if (a.n == 0) return FPG_OK;
+    cell_index_kernel<<<(a.n + 255) / 256, 256, 0, ctx->pick(stream)>>>(a, lt, out_dev);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_grid_download(fpg_grid* g, uint32_t* counts, uint32_t* mass_scaled, float* mass_kg,
+                                        void* stream) {
+    if (!g) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = g->ctx->pick(stream);
+    const size_t cells = g->nx * g->ny * g->nz;
+    if (counts) FPG_CUDA(cudaMemcpyAsync(counts, g->counts, cells * 4, cudaMemcpyDeviceToHost, s));
+    uint32_t* ms = mass_scaled;
+    uint32_t* tmp = nullptr;
+    if (!ms && mass_kg) {
+        tmp = new uint32_t[cells];
+        ms = tmp;
+    }
+    cudaError_t e = cudaSuccess;
+    if (ms) e = cudaMemcpyAsync(ms, g->mass, cells * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && mass_kg) {
+        // download_output (gridding.rs:210-213): (value as f32) / mass_scale
+        for (size_t i = 0; i < cells; ++i) mass_kg[i] = (float)ms[i] / g->mass_scale;
+    }
+    delete[] tmp;
+    return e == cudaSuccess ? FPG_OK : cuda_status(e);
+}
+
+extern "C" uint32_t* fpg_grid_counts_device(fpg_grid* g) { return g ? g->counts : nullptr; }
+extern "C" uint32_t* fpg_grid_mass_device(fpg_grid* g) { return g ? g->mass : nullptr; }

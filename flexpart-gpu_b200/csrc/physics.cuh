@@ -1,0 +1,221 @@
+// physics.cuh — per-particle device physics of the flexpart-gpu step.
+//
+// One __device__ function per reference routine, each citing the WGSL shader
+// (the reference GPU path) and the Rust CPU routine it restates.  All code is
+// compiled with -fmad=false: every multiply and add rounds separately, exactly
+// as written, and the only fused operation is the explicit fmaf of lerp()
+// (the reference CPU lerp is `a.mul_add(1 - t, b * t)`,
+// src/physics/interpolation.rs:75-77, src/io/temporal.rs:417-420).
+// Transcendentals are CUDA's IEEE-accurate expf/logf/powf/sinf/cosf; sqrtf
+// and '/' are correctly rounded (no fast-math flags).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fpg {
+
+constexpr uint32_t FLAG_ACTIVE = 1u;
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+__device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(a, 1.0f - t, b * t); }
+__device__ __forceinline__ float sanitize_positive(float v) { return (finitef(v) && v > 0.0f) ? v : 0.0f; }
+
+// ---- Philox4x32-10 (src/physics/rng.rs:28-65, langevin_fused.wgsl:126-169) --
+struct u32x4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = u32x4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// counter_add with a u32 offset (langevin_fused.wgsl:171-180).
+__device__ __forceinline__ u32x4 counter_add(u32x4 b, uint32_t offset) {
+    u32x4 r;
+    r.x = b.x + offset;
+    const uint32_t c0 = r.x < b.x;
+    r.y = b.y + c0;
+    const uint32_t c1 = (c0 == 1u) && (r.y < b.y);
+    r.z = b.z + c1;
+    const uint32_t c2 = (c1 == 1u) && (r.z < b.z);
+    r.w = b.w + c2;
+    return r;
+}
+
+// u32_to_uniform01 (rng.rs:94-96).
+__device__ __forceinline__ float u32_to_uniform01(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216.0f); }
+
+// box_muller_normals (physics/langevin.rs:176-182, langevin_fused.wgsl:186-192).
+__device__ __forceinline__ float2 box_muller(float u0, float u1) {
+    const float ru = clampf(u0, 1.17549435e-38f, 0.99999994f);
+    const float au = clampf(u1, 0.0f, 0.99999994f);
+    const float radius = sqrtf(-2.0f * logf(ru));
+    const float theta = 6.2831855f * au;
+    return make_float2(radius * cosf(theta), radius * sinf(theta));
+}
+
+// ---- Hanna (physics/hanna.rs:49-163, langevin_fused.wgsl:224-293) ----------
+struct Hanna {
+    float ust, wst, ol, h;
+    float sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
+};
+
+__device__ __forceinline__ float obukhov_from_inverse(float oli) {
+    // hanna.rs:169-174: |1/L| < 1e-5 is neutral (L = +inf).
+    return fabsf(oli) < 1.0e-5f ? __int_as_float(0x7f800000) : 1.0f / oli;
+}
+
+__device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float ol, float h_in, float z_in) {
+    Hanna o;
+    const float ust = fmaxf(ust_in, 1.0e-4f);
+    const float wst = fmaxf(wst_in, 0.0f);
+    const float h = fmaxf(h_in, 1.0f);
+    const float z = clampf(z_in, 0.0f, h);
+    const float zeta = clampf(z / h, 0.0f, 1.0f);
+    float sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
+    if (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) {
+        const float corr = z / ust;
+        sigu = 1.0e-2f + 2.0f * ust * expf(-3.0e-4f * corr);
+        sigw = 1.3f * ust * expf(-2.0e-4f * corr);
+        dsigwdz = -2.0e-4f * sigw;
+        sigw = sigw + 1.0e-2f;
+        sigv = sigw;
+        tlu = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
+        tlv = tlu;
+        tlw = tlu;
+    } else if (ol < 0.0f) {
+        sigu = 1.0e-2f + ust * powf(12.0f - 0.5f * h / ol, 1.0f / 3.0f);
+        sigv = sigu;
+        const float z23 = powf(zeta, 2.0f / 3.0f);
+        const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
+        sigw = sqrtf(sigw_sq) + 1.0e-2f;
+        dsigwdz = 0.5f / sigw / h *
+                  (-1.4f * ust * ust + wst * wst * (0.8f * powf(fmaxf(zeta, 1.0e-3f), -(1.0f / 3.0f)) - 1.8f * z23));
+        tlu = 0.15f * h / sigu;
+        tlv = tlu;
+        if (z < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * fabsf(z / ol)));
+        else if (zeta < 0.1f) tlw = 0.59f * z / sigw;
+        else tlw = 0.15f * h / sigw * (1.0f - expf(-5.0f * zeta));
+    } else {
+        sigu = 1.0e-2f + 2.0f * ust * (1.0f - zeta);
+        sigv = 1.0e-2f + 1.3f * ust * (1.0f - zeta);
+        sigw = sigv;
+        dsigwdz = -1.3f * ust / h;
+        tlu = 0.15f * h / sigu * sqrtf(zeta);
+        tlv = 0.467f * tlu;
+        tlw = 0.1f * h / sigw * powf(zeta, 0.8f);
+    }
+    tlu = fmaxf(tlu, 10.0f);
+    tlv = fmaxf(tlv, 10.0f);
+    tlw = fmaxf(tlw, 30.0f);
+    if (dsigwdz == 0.0f) dsigwdz = 1.0e-10f;
+    if (!finitef(sigu) || sigu <= 0.0f) sigu = 1.0e-2f;
+    if (!finitef(sigv) || sigv <= 0.0f) sigv = 1.0e-2f;
+    if (!finitef(sigw) || sigw <= 0.0f) sigw = 1.0e-2f;
+    if (!finitef(tlu)) tlu = 10.0f;
+    if (!finitef(tlv)) tlv = 10.0f;
+    if (!finitef(tlw)) tlw = 30.0f;
+    if (!finitef(dsigwdz)) dsigwdz = 1.0e-10f;
+    o.ust = ust; o.wst = wst; o.ol = ol; o.h = h;
+    o.sigu = sigu; o.sigv = sigv; o.sigw = sigw; o.dsigwdz = dsigwdz;
+    o.tlu = tlu; o.tlv = tlv; o.tlw = tlw;
+    return o;
+}
+
+// hanna_short_w (langevin_fused.wgsl:296-344): sigw, dsigwdz, tlw at a new
+// height.  ust, wst, h are the already-floored values of compute_hanna.
+__device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float ol, float h_in, float z_in,
+                                              float& sigw_o, float& dsigwdz_o, float& tlw_o) {
+    const float ust = fmaxf(ust_in, 1.0e-4f);
+    const float wst = fmaxf(wst_in, 0.0f);
+    const float h = fmaxf(h_in, 1.0f);
+    const float z = clampf(z_in, 0.0f, h);
+    const float zeta = clampf(z / h, 0.0f, 1.0f);
+    float sigw, dsigwdz, tlw;
+    if (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) {
+        const float corr = z / ust;
+        sigw = 1.3f * ust * expf(-2.0e-4f * corr);
+        dsigwdz = -2.0e-4f * sigw;
+        sigw = sigw + 1.0e-2f;
+        tlw = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
+    } else if (ol < 0.0f) {
+        const float z23 = powf(zeta, 2.0f / 3.0f);
+        const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
+        sigw = sqrtf(sigw_sq) + 1.0e-2f;
+        dsigwdz = 0.5f / sigw / h *
+                  (-1.4f * ust * ust + wst * wst * (0.8f * powf(fmaxf(zeta, 1.0e-3f), -(1.0f / 3.0f)) - 1.8f * z23));
+        if (z < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * fabsf(z / ol)));
+        else if (zeta < 0.1f) tlw = 0.59f * z / sigw;
+        else tlw = 0.15f * h / sigw * (1.0f - expf(-5.0f * zeta));
+    } else {
+        sigw = 1.0e-2f + 1.3f * ust * (1.0f - zeta);
+        dsigwdz = -1.3f * ust / h;
+        tlw = 0.1f * h / sigw * powf(zeta, 0.8f);
+    }
+    tlw = fmaxf(tlw, 30.0f);
+    if (dsigwdz == 0.0f) dsigwdz = 1.0e-10f;
+    if (!finitef(sigw) || sigw <= 0.0f) sigw = 1.0e-2f;
+    if (!finitef(tlw)) tlw = 30.0f;
+    if (!finitef(dsigwdz)) dsigwdz = 1.0e-10f;
+    sigw_o = sigw; dsigwdz_o = dsigwdz; tlw_o = tlw;
+}
+
+// ---- Langevin OU updates (physics/langevin.rs:116-170, langevin_fused.wgsl:350-389)
+__device__ __forceinline__ float langevin_h(float prev, float sigma_in, float tl_in, float dt, float eta) {
+    const float sigma = sanitize_positive(sigma_in);
+    const float tl = sanitize_positive(tl_in);
+    if (tl == 0.0f) return 0.0f;
+    const float ratio = dt / tl;
+    float next;
+    if (ratio < 0.5f) {
+        next = (1.0f - ratio) * prev + eta * sigma * sqrtf(fmaxf(2.0f * ratio, 0.0f));
+    } else {
+        const float corr = expf(-ratio);
+        next = corr * prev + eta * sigma * sqrtf(fmaxf(1.0f - corr * corr, 0.0f));
+    }
+    return finitef(next) ? next : 0.0f;
+}
+
+__device__ __forceinline__ float langevin_v(float prev, float sigw_in, float tlw_in, float dsigwdz, float dt,
+                                            float rho, float eta) {
+    const float sigma_w = sanitize_positive(sigw_in);
+    const float tlw = sanitize_positive(tlw_in);
+    if (tlw == 0.0f) return 0.0f;
+    const float drift = sigma_w * (dsigwdz + rho * sigma_w);
+    const float ratio = dt / tlw;
+    float next;
+    if (ratio < 0.5f) {
+        next = (1.0f - ratio) * prev + eta * sigma_w * sqrtf(fmaxf(2.0f * ratio, 0.0f)) + dt * drift;
+    } else {
+        const float corr = expf(-ratio);
+        next = corr * prev + eta * sigma_w * sqrtf(fmaxf(1.0f - corr * corr, 0.0f)) + tlw * (1.0f - corr) * drift;
+    }
+    return finitef(next) ? next : 0.0f;
+}
+
+// ---- Deposition --------------------------------------------------------------
+// dry_deposition.wgsl:70-74 (survival factor; href already floored at 0.1 m).
+__device__ __forceinline__ float dry_survival(float vdep, float dt, float href) {
+    const float exponent = -fmaxf(vdep, 0.0f) * fabsf(dt) / (2.0f * href);
+    return clampf(expf(exponent), 0.0f, 1.0f);
+}
+
+// wet_deposition.wgsl:179-188, physics/wet_scavenging.rs:375-384.
+__device__ __forceinline__ float wet_probability(float lambda_in, float dt_in, float fraction_in) {
+    const float lambda = fmaxf(lambda_in, 0.0f);
+    const float dt = fabsf(dt_in);
+    const float fraction = clampf(fraction_in, 0.0f, 1.0f);
+    if (lambda <= 0.0f || dt <= 0.0f || fraction <= 0.0f) return 0.0f;
+    const float local = 1.0f - expf(-lambda * dt);
+    return clampf(local * fraction, 0.0f, 1.0f);
+}
+
+}  // namespace fpg

@@ -1,0 +1,917 @@
+// step.cu — the fused per-particle step and the per-cell kernels around it.
+//
+// fused_step_kernel is the B200 replacement of four reference compute passes
+// encoded back to back by ForwardTimeLoopDriver::run_timestep
+// (src/simulation/timeloop.rs:1095-1180):
+//   advection_dual_wind.wgsl:254-303  (Petterssen with dual-time wind)
+//   langevin_fused.wgsl:402-518        (Hanna + Langevin, sub-steps, reflection)
+//   dry_deposition.wgsl:76-106         (mass decay in the surface layer)
+//   wet_deposition.wgsl:190-217        (below-cloud scavenging)
+// Each reference pass reads and writes the whole 96-byte particle; here each
+// particle's structure-of-arrays fields are read once and written once
+// (96 B per particle-step with one species), and the four passes' math runs
+// in registers in between.
+//
+// Data layout in HBM:
+//   particles: one 4-byte array per field, slot-indexed (coalesced 128-B
+//     warp accesses);
+//   wind bracket: node-major float4 pairs, t0 at [2n] and t1 at [2n+1]
+//     (u, v, w, 0) so the 8 corners of a sample cost 16 16-byte loads;
+//   PBL: float4 (u*, w*, hmix, 1/L) per met cell, one 16-byte gather per
+//     particle;
+//   wet forcing per cell: float2 (lambda, fraction).
+// Level heights sit in shared memory; the metres->level search is a binary
+// search when heights are non-decreasing (same first index as the
+// reference's linear scan, advection_dual_wind.wgsl:94-117), else the scan.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "fpg_internal.h"
+#include "physics.cuh"
+
+namespace fpg {
+
+struct StepArgs {
+    int32_t* cell_x; int32_t* cell_y;
+    float* pos_x; float* pos_y; float* pos_z;
+    const uint32_t* flags;
+    float* mass[4];
+    float* vel_u; float* vel_v; float* vel_w;
+    float* turb_u; float* turb_v; float* turb_w;
+    int32_t* cbt;
+    uint32_t n;
+    int n_species;
+    uint32_t stages;
+    // advection
+    const float4* bracket;
+    const float* heights;
+    uint32_t nx, ny, nz;
+    int has_heights, monotonic;
+    float alpha, dt, xs, ys, zs;
+    // turbulence
+    const float4* pbl;
+    uint32_t pnx, pny;
+    float tdt, rho, zmin;
+    uint32_t n_sub;
+    uint32_t key0, key1;
+    u32x4 counter;
+    // deposition
+    float href;
+    int dry_mode;
+    float dry_v;
+    const float* dry_v_arr;
+    float* dry_prob;
+    int wet_mode;
+    float wet_l, wet_f;
+    const float* wet_l_arr;
+    const float* wet_f_arr;
+    const float2* wet_cells;
+    uint32_t wnx, wny;
+    float* wet_prob;
+};
+
+// meters_to_grid_level (advection_dual_wind.wgsl:94-117).
+__device__ __forceinline__ float meters_to_level(const float* h, uint32_t nz, int has, int mono, float z) {
+    if (!has) return z;
+    const float h0 = h[0];
+    if (z <= h0) return h0 > 0.0f ? z / h0 : 0.0f;
+    uint32_t k;
+    if (mono) {
+        // first k in [1, nz) with z <= h[k]; nz if none
+        uint32_t lo = 1u, hi = nz;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (z <= h[mid]) hi = mid; else lo = mid + 1u;
+        }
+        k = lo;
+    } else {
+        k = nz;
+        for (uint32_t i = 1u; i < nz; ++i) if (z <= h[i]) { k = i; break; }
+    }
+    if (k >= nz) return (float)(nz - 1u);
+    const float hprev = h[k - 1u];
+    const float denom = h[k] - hprev;
+    if (denom > 0.0f) return (float)(k - 1u) + (z - hprev) / denom;
+    return (float)(k - 1u);
+}
+
+// clamp_axis (advection_dual_wind.wgsl:130-138).
+__device__ __forceinline__ void axis_bracket(float coord, uint32_t n, uint32_t& lo, uint32_t& hi, float& t) {
+    const float c = clampf(coord, 0.0f, (float)(n - 1u));
+    const float lf = floorf(c);
+    lo = (uint32_t)lf;
+    hi = min(lo + 1u, n - 1u);
+    t = c - lf;
+}
+
+__device__ __forceinline__ float tri(float c000, float c100, float c010, float c110, float c001, float c101,
+                                     float c011, float c111, float tx, float ty, float tz) {
+    return lerpf(lerpf(lerpf(c000, c100, tx), lerpf(c010, c110, tx), ty),
+                 lerpf(lerpf(c001, c101, tx), lerpf(c011, c111, tx), ty), tz);
+}
+
+// sample_dual_{u,v,w} (advection_dual_wind.wgsl:142-236): trilinear in each
+// frame, then lerp by alpha.
+__device__ __forceinline__ float3 sample_dual(const StepArgs& a, const float* hts, float x, float y, float z) {
+    uint32_t x0, x1, y0, y1, z0, z1;
+    float tx, ty, tz;
+    axis_bracket(x, a.nx, x0, x1, tx);
+    axis_bracket(y, a.ny, y0, y1, ty);
+    axis_bracket(meters_to_level(hts, a.nz, a.has_heights, a.monotonic, z), a.nz, z0, z1, tz);
+    const uint32_t c00 = (x0 * a.ny + y0) * a.nz, c10 = (x1 * a.ny + y0) * a.nz;
+    const uint32_t c01 = (x0 * a.ny + y1) * a.nz, c11 = (x1 * a.ny + y1) * a.nz;
+    const float4* br = a.bracket;
+    const float4 p000 = __ldg(br + 2u * (c00 + z0)), q000 = __ldg(br + 2u * (c00 + z0) + 1u);
+    const float4 p100 = __ldg(br + 2u * (c10 + z0)), q100 = __ldg(br + 2u * (c10 + z0) + 1u);
+    const float4 p010 = __ldg(br + 2u * (c01 + z0)), q010 = __ldg(br + 2u * (c01 + z0) + 1u);
+    const float4 p110 = __ldg(br + 2u * (c11 + z0)), q110 = __ldg(br + 2u * (c11 + z0) + 1u);
+    const float4 p001 = __ldg(br + 2u * (c00 + z1)), q001 = __ldg(br + 2u * (c00 + z1) + 1u);
+    const float4 p101 = __ldg(br + 2u * (c10 + z1)), q101 = __ldg(br + 2u * (c10 + z1) + 1u);
+    const float4 p011 = __ldg(br + 2u * (c01 + z1)), q011 = __ldg(br + 2u * (c01 + z1) + 1u);
+    const float4 p111 = __ldg(br + 2u * (c11 + z1)), q111 = __ldg(br + 2u * (c11 + z1) + 1u);
+    float3 r;
+    r.x = lerpf(tri(p000.x, p100.x, p010.x, p110.x, p001.x, p101.x, p011.x, p111.x, tx, ty, tz),
+                tri(q000.x, q100.x, q010.x, q110.x, q001.x, q101.x, q011.x, q111.x, tx, ty, tz), a.alpha);
+    r.y = lerpf(tri(p000.y, p100.y, p010.y, p110.y, p001.y, p101.y, p011.y, p111.y, tx, ty, tz),
+                tri(q000.y, q100.y, q010.y, q110.y, q001.y, q101.y, q011.y, q111.y, tx, ty, tz), a.alpha);
+    r.z = lerpf(tri(p000.z, p100.z, p010.z, p110.z, p001.z, p101.z, p011.z, p111.z, tx, ty, tz),
+                tri(q000.z, q100.z, q010.z, q110.z, q001.z, q101.z, q011.z, q111.z, tx, ty, tz), a.alpha);
+    return r;
+}
+
+// split_horizontal_coord (advection_dual_wind.wgsl:238-248).
+__device__ __forceinline__ void split_coord(float coord, uint32_t n, int32_t& cell, float& frac) {
+    const float c = clampf(coord, 0.0f, (float)(n - 1u));
+    uint32_t ci = (uint32_t)floorf(c);
+    float f = c - (float)ci;
+    if (ci >= n - 1u) { ci = n - 1u; f = 0.0f; }
+    cell = (int32_t)ci;
+    frac = f;
+}
+
+__global__ void __launch_bounds__(256) fused_step_kernel(StepArgs a) {
+    extern __shared__ float s_heights[];
+    if (a.stages & FPG_STAGE_ADVECT) {
+        for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
+        __syncthreads();
+    }
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const bool dry_on = (a.stages & FPG_STAGE_DRY) && a.dry_mode != FPG_FORCING_NONE;
+    const bool wet_on = (a.stages & FPG_STAGE_WET) && a.wet_mode != FPG_FORCING_NONE;
+    if (!(a.flags[p] & FLAG_ACTIVE)) {
+        if (dry_on && a.dry_prob) a.dry_prob[p] = 0.0f;
+        if (wet_on && a.wet_prob) a.wet_prob[p] = 0.0f;
+        return;
+    }
+    int32_t cx = a.cell_x[p], cy = a.cell_y[p];
+    float px = a.pos_x[p], py = a.pos_y[p], pz = a.pos_z[p];
+    const bool turb_on = (a.stages & FPG_STAGE_TURBULENCE) != 0;
+    float tu = a.turb_u[p], tv = a.turb_v[p];
+
+    // ---- advection_dual_wind.wgsl:266-300 ----
+    if (a.stages & FPG_STAGE_ADVECT) {
+        const float x0 = (float)cx + px;
+        const float y0 = (float)cy + py;
+        const float z0 = pz;
+        const float3 s0 = sample_dual(a, s_heights, x0, y0, z0);
+        const float u0 = s0.x + tu, v0 = s0.y + tv, w0 = s0.z;
+        const float xmax = (float)(a.nx - 1u), ymax = (float)(a.ny - 1u);
+        const float ztop = a.has_heights ? s_heights[a.nz - 1u] : (float)(a.nz - 1u);
+        const float pxp = clampf(x0 + (u0 * a.xs) * a.dt, 0.0f, xmax);
+        const float pyp = clampf(y0 + (v0 * a.ys) * a.dt, 0.0f, ymax);
+        const float pzp = clampf(z0 + (w0 * a.zs) * a.dt, 0.0f, ztop);
+        const float3 s1 = sample_dual(a, s_heights, pxp, pyp, pzp);
+        const float u1 = s1.x + tu, v1 = s1.y + tv, w1 = s1.z;
+        const float cu = 0.5f * (u0 + u1), cv = 0.5f * (v0 + v1), cw = 0.5f * (w0 + w1);
+        const float x1 = clampf(x0 + (cu * a.xs) * a.dt, 0.0f, xmax);
+        const float y1 = clampf(y0 + (cv * a.ys) * a.dt, 0.0f, ymax);
+        pz = clampf(z0 + (cw * a.zs) * a.dt, 0.0f, ztop);
+        split_coord(x1, a.nx, cx, px);
+        split_coord(y1, a.ny, cy, py);
+        a.cell_x[p] = cx; a.cell_y[p] = cy;
+        a.pos_x[p] = px; a.pos_y[p] = py;
+        a.vel_u[p] = cu; a.vel_v[p] = cv; a.vel_w[p] = cw;
+    }
+
+    // ---- langevin_fused.wgsl:414-515 ----
+    if (turb_on) {
+        const float x = (float)cx + px;
+        const float y = (float)cy + py;
+        const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(a.pnx - 1u)));
+        const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(a.pny - 1u)));
+        const float4 cell = __ldg(a.pbl + (i * a.pny + j));
+        const Hanna hn = compute_hanna(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
+
+        const uint32_t n_vert = a.n_sub > 1u ? a.n_sub : 1u;
+        const uint32_t blocks = (2u + n_vert + 3u) / 4u;
+        const u32x4 b0 = philox4x32_10(counter_add(a.counter, p * blocks), a.key0, a.key1);
+        u32x4 b1 = {0u, 0u, 0u, 0u};
+        if (blocks > 1u) b1 = philox4x32_10(counter_add(a.counter, p * blocks + 1u), a.key0, a.key1);
+        const float2 e_uv = box_muller(u32_to_uniform01(b0.x), u32_to_uniform01(b0.y));
+        const float2 e_w01 = box_muller(u32_to_uniform01(b0.z), u32_to_uniform01(b0.w));
+        const float2 e_w23 = box_muller(u32_to_uniform01(b1.x), u32_to_uniform01(b1.y));
+
+        tu = langevin_h(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
+        tv = langevin_h(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
+        float tw = a.turb_w[p];
+        if (a.n_sub == 0u) {
+            tw = langevin_v(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
+        } else {
+            int32_t cbt = a.cbt[p];
+            const int32_t cbt_in = cbt;
+            const float dt_sub = a.tdt / (float)a.n_sub;
+            const float h = hn.h;
+            const float zmin = a.zmin;
+            float sigw = hn.sigw, dsigwdz = hn.dsigwdz, tlw = hn.tlw;
+            for (uint32_t sub = 0; sub < a.n_sub; ++sub) {
+                const float eta = sub == 0u ? e_w01.x : sub == 1u ? e_w01.y : sub == 2u ? e_w23.x : e_w23.y;
+                tw = langevin_v(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
+                pz = pz + tw * dt_sub;
+                if (h > zmin) {
+                    float z = pz;
+                    for (int bounce = 0; bounce < 10; ++bounce) {
+                        if (z < zmin) { z = 2.0f * zmin - z; cbt = -cbt; tw = -tw; }
+                        else if (z > h) { z = 2.0f * h - z; cbt = -cbt; tw = -tw; }
+                        else break;
+                    }
+                    pz = clampf(z, zmin, h);
+                }
+                if (sub < a.n_sub - 1u) hanna_short_w(hn.ust, hn.wst, hn.ol, hn.h, pz, sigw, dsigwdz, tlw);
+            }
+            if (cbt != cbt_in) a.cbt[p] = cbt;
+        }
+        a.turb_u[p] = tu; a.turb_v[p] = tv; a.turb_w[p] = tw;
+    }
+    if ((a.stages & FPG_STAGE_ADVECT) || (turb_on && a.n_sub != 0u)) a.pos_z[p] = pz;
+
+    // ---- dry_deposition.wgsl:89-105 and wet_deposition.wgsl:203-216 ----
+    if (dry_on || wet_on) {
+        float survival = 1.0f;
+        if (dry_on) {
+            float prob = 0.0f;
+            if (!(pz >= 2.0f * a.href)) {
+                const float vd = a.dry_mode == FPG_FORCING_PER_PARTICLE ? a.dry_v_arr[p] : a.dry_v;
+                const float s = dry_survival(vd, a.tdt, a.href);
+                prob = 1.0f - s;
+                survival = s;
+            }
+            if (a.dry_prob) a.dry_prob[p] = prob;
+        }
+        float wsurv = 1.0f;
+        if (wet_on) {
+            float lam, fr;
+            if (a.wet_mode == FPG_FORCING_PER_PARTICLE) {
+                lam = a.wet_l_arr[p]; fr = a.wet_f_arr[p];
+            } else if (a.wet_mode == FPG_FORCING_PER_CELL) {
+                const float x = (float)cx + px;
+                const float y = (float)cy + py;
+                const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(a.wnx - 1u)));
+                const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(a.wny - 1u)));
+                const float2 c = __ldg(a.wet_cells + (i * a.wny + j));
+                lam = c.x; fr = c.y;
+            } else {
+                lam = a.wet_l; fr = a.wet_f;
+            }
+            const float prob = wet_probability(lam, a.tdt, fr);
+            wsurv = 1.0f - prob;
+            if (a.wet_prob) a.wet_prob[p] = prob;
+        }
+        // mass * dry survival, then * wet survival: two roundings, as the
+        // two reference passes apply them.
+        for (int k = 0; k < a.n_species; ++k) {
+            float m = a.mass[k][p];
+            if (dry_on && !(pz >= 2.0f * a.href)) m = m * survival;
+            if (wet_on) m = m * wsurv;
+            a.mass[k][p] = m;
+        }
+    }
+}
+
+// ---- per-cell kernels --------------------------------------------------------
+
+__device__ __forceinline__ float sp_(float v, float fb) { return (finitef(v) && v > 0.0f) ? v : fb; }
+__device__ __forceinline__ float snn_(float v, float fb) { return (finitef(v) && v >= 0.0f) ? v : fb; }
+__device__ __forceinline__ float sf_(float v, float fb) { return finitef(v) ? v : fb; }
+
+// interpolate_surface_fields_linear (io/temporal.rs:99-104,122-214) followed
+// by pbl_diagnostics.wgsl:238-305 for one cell.
+__global__ void __launch_bounds__(256) pbl_diag_kernel(const fpg_surface_cell* __restrict__ s0,
+                                                       const fpg_surface_cell* __restrict__ s1, float alpha,
+                                                       fpg_pbl_options o, uint32_t ncell, float* ustar_o,
+                                                       float* wstar_o, float* hmix_o, float* oli_o, float* sshf_o,
+                                                       float* ssr_o, float* surfstr_o, float4* packed) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    float in[10];
+    const float* a = &s0[c].surface_pressure_pa;
+    const float* b = &s1[c].surface_pressure_pa;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        if (alpha <= 0.0f) in[k] = a[k];
+        else if (alpha >= 1.0f) in[k] = b[k];
+        else in[k] = lerpf(a[k], b[k], alpha);
+    }
+    const float sp = in[0], t2 = in[1], u10 = in[2], v10 = in[3], stress = in[4], shf = in[5], ssr = in[6];
+    const float hm = in[7], fv = in[8], oli_in = in[9];
+    const float temp_k = sp_(t2, 300.0f);
+    const float pressure = sp_(sp, 101325.0f);
+    const float air_density = pressure / (287.05f * temp_k);
+    float est;
+    {
+        const float rho = sp_(air_density, 1.225f);
+        const float safe_stress = snn_(stress, 0.0f);
+        if (safe_stress > 0.0f) {
+            est = fmaxf(sqrtf(safe_stress / rho), 1.0e-4f);
+        } else {
+            const float z0 = sp_(o.roughness_length_m, 0.1f);
+            const float zr = fmaxf(sp_(o.wind_reference_height_m, 10.0f), 1.01f * z0);
+            const float ws = fmaxf(sqrtf(u10 * u10 + v10 * v10), 0.0f);
+            if (ws <= 0.0f) {
+                est = 1.0e-4f;
+            } else {
+                const float us = 0.4f * ws / fmaxf(logf(zr / z0), 1.0e-6f);
+                est = fmaxf(sp_(us, 1.0e-4f), 1.0e-4f);
+            }
+        }
+    }
+    const float ustar = (finitef(fv) && fv > 0.0f) ? fmaxf(fv, 1.0e-4f) : fmaxf(est, 1.0e-4f);
+    float computed_ol;
+    {
+        const float hf = sf_(shf, 0.0f);
+        if (fabsf(hf) < fmaxf(o.heat_flux_neutral_threshold_w_m2, 0.0f)) {
+            computed_ol = __int_as_float(0x7f800000);
+        } else {
+            const float u = fmaxf(sp_(ustar, 1.0e-4f), 1.0e-4f);
+            const float t = sp_(temp_k, 300.0f);
+            const float d = sp_(air_density, 1.225f);
+            const float numerator = -(d * 1004.6f * t * u * u * u);
+            const float denominator = 0.4f * 9.81f * hf;
+            if (fabsf(denominator) < 1.0e-9f) {
+                computed_ol = __int_as_float(0x7f800000);
+            } else {
+                const float olv = numerator / denominator;
+                computed_ol = (!finitef(olv) || fabsf(olv) > 1.0e9f) ? __int_as_float(0x7f800000) : olv;
+            }
+        }
+    }
+    float oli;
+    if (finitef(oli_in) && fabsf(oli_in) >= 1.0e-5f) oli = oli_in;
+    else oli = (!finitef(computed_ol) || fabsf(computed_ol) > 1.0e5f) ? 0.0f : 1.0f / computed_ol;
+    const float hsrc = (finitef(hm) && hm > 0.0f) ? hm : o.fallback_mixing_height_m;
+    const float hmix = fmaxf(clampf(hsrc, o.hmix_min_m, o.hmix_max_m), o.hmix_min_m);
+    const float safe_shf = sf_(shf, 0.0f);
+    float wstar = 0.0f;
+    if (safe_shf > 0.0f) {
+        const float d = sp_(air_density, 1.225f);
+        const float t = sp_(temp_k, 300.0f);
+        const float hh = sp_(hmix, o.hmix_min_m);
+        const float bf = safe_shf / (d * 1004.6f) * 9.81f / t;
+        if (!(bf <= 0.0f || !finitef(bf))) wstar = fmaxf(powf(bf * hh, 1.0f / 3.0f), 0.0f);
+    }
+    ustar_o[c] = ustar; wstar_o[c] = wstar; hmix_o[c] = hmix; oli_o[c] = oli;
+    sshf_o[c] = sf_(shf, 0.0f);
+    ssr_o[c] = snn_(ssr, 0.0f);
+    surfstr_o[c] = snn_(stress, 0.0f);
+    packed[c] = make_float4(ustar, wstar, hmix, oli);
+}
+
+__global__ void __launch_bounds__(256) pack_pbl_kernel(const float* __restrict__ u, const float* __restrict__ w,
+                                                       const float* __restrict__ h, const float* __restrict__ o,
+                                                       uint32_t ncell, float4* packed) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncell) packed[c] = make_float4(u[c], w[c], h[c], o[c]);
+}
+
+__global__ void __launch_bounds__(256) pack_frame_kernel(const float* __restrict__ u, const float* __restrict__ v,
+                                                         const float* __restrict__ w, uint32_t nodes, int which,
+                                                         float4* bracket) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < nodes) bracket[2u * n + (uint32_t)which] = make_float4(u[n], v[n], w[n], 0.0f);
+}
+
+__device__ __forceinline__ float snn0(float v) { return (finitef(v) && v > 0.0f) ? v : 0.0f; }
+__device__ __forceinline__ int precip_class(float p) {
+    return p > 20.0f ? 4 : p > 8.0f ? 3 : p > 3.0f ? 2 : p > 1.0f ? 1 : 0;
+}
+
+// wet_precipitation_state + below_cloud_scavenging_coefficient_gas
+// (physics/wet_scavenging.rs:179-225,78-82) per met cell.
+__global__ void __launch_bounds__(256) wet_cells_kernel(const float* __restrict__ lsp_in,
+                                                        const float* __restrict__ conv_in,
+                                                        const float* __restrict__ cc_in, float a_in, float b_in,
+                                                        uint32_t ncell, float2* out) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const float lsf[5] = {0.5f, 0.65f, 0.8f, 0.9f, 0.95f};
+    const float cvf[5] = {0.4f, 0.55f, 0.7f, 0.8f, 0.9f};
+    const float lsp = snn0(lsp_in[c]), convp = snn0(conv_in[c]);
+    const float total = lsp + convp;
+    float fraction = 0.0f, subgrid = 0.0f;
+    if (!(total < 0.01f)) {
+        const float cc = clampf(cc_in[c], 0.0f, 1.0f);
+        const float weighted = (lsp * lsf[precip_class(lsp)] + convp * cvf[precip_class(convp)]) / fmaxf(total, 1.0e-12f);
+        const float area = fminf(fmaxf(fmaxf(cc * weighted, 0.05f), 0.05f), 1.0f);
+        subgrid = snn0(total / fmaxf(area, 1.0e-12f));
+        fraction = area;
+    }
+    float lambda = 0.0f;
+    if (total >= 0.01f && fraction > 0.0f && subgrid > 0.0f) {
+        lambda = snn0(snn0(a_in) * powf(subgrid, snn0(b_in)));
+    } else {
+        fraction = 0.0f;
+    }
+    out[c] = make_float2(lambda, fraction);
+}
+
+__global__ void __launch_bounds__(256) fill_kernel(float* out, uint32_t n, float v) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = v;
+}
+
+__global__ void __launch_bounds__(256) philox_kernel(uint32_t k0, uint32_t k1, u32x4 base, uint32_t n_blocks,
+                                                     float* out, uint32_t* raw) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n_blocks) return;
+    // philox_rng.wgsl: block b uses counter base + b (64-bit add as rng.rs:69-87)
+    u32x4 c = counter_add(base, b);
+    const u32x4 r = philox4x32_10(c, k0, k1);
+    if (out) {
+        out[4u * b + 0u] = u32_to_uniform01(r.x); out[4u * b + 1u] = u32_to_uniform01(r.y);
+        out[4u * b + 2u] = u32_to_uniform01(r.z); out[4u * b + 3u] = u32_to_uniform01(r.w);
+    }
+    if (raw) { raw[4u * b] = r.x; raw[4u * b + 1u] = r.y; raw[4u * b + 2u] = r.z; raw[4u * b + 3u] = r.w; }
+}
+
+static inline uint32_t blocks_for(size_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+}  // namespace fpg
+
+using namespace fpg;
+
+// ============================================================================
+// C ABI: met, PBL, surface, cell fields
+// ============================================================================
+
+extern "C" fpg_status fpg_met_create(fpg_ctx* ctx, size_t nx, size_t ny, size_t nz, fpg_met** out) {
+    if (!ctx || !out) return FPG_ERR_INVALID_ARGUMENT;
+    if (nx == 0 || ny == 0 || nz == 0) return FPG_ERR_ZERO_SHAPE;
+    if (nz > FPG_MAX_LEVELS) return FPG_ERR_TOO_MANY_LEVELS;
+    const size_t nodes = nx * ny * nz;
+    if (nodes * 2 >= (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    fpg_met* m = new fpg_met();
+    m->ctx = ctx; m->nx = nx; m->ny = ny; m->nz = nz;
+    cudaError_t e = cudaMalloc(&m->bracket, nodes * 2 * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc(&m->staging, nodes * 3 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->heights_dev, nz * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->bracket, 0, nodes * 2 * sizeof(float4), ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->heights_dev, 0, nz * sizeof(float), ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(m->bracket); cudaFree(m->staging); cudaFree(m->heights_dev); delete m;
+        return cuda_status(e);
+    }
+    *out = m;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_met_destroy(fpg_met* m) {
+    if (!m) return FPG_OK;
+    cudaFree(m->bracket);
+    cudaFree(m->staging);
+    cudaFree(m->heights_dev);
+    delete m;
+    return FPG_OK;
+}
+
+static fpg_status met_pack(fpg_met* m, int which, const float* u, const float* v, const float* w, cudaStream_t s) {
+    const uint32_t nodes = (uint32_t)(m->nx * m->ny * m->nz);
+    pack_frame_kernel<<<blocks_for(nodes, 256), 256, 0, s>>>(u, v, w, nodes, which, m->bracket);
+    m->ctx->count();
+    FPG_CHECK_LAUNCH();
+    m->uploaded[which] = true;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_met_upload_frame(fpg_met* m, int32_t which, const float* u, const float* v,
+                                           const float* w, void* stream) {
+    if (!m || !u || !v || !w || (which != 0 && which != 1)) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = m->ctx->pick(stream);
+    const size_t nodes = m->nx * m->ny * m->nz;
+    FPG_CUDA(cudaMemcpyAsync(m->staging, u, nodes * sizeof(float), cudaMemcpyHostToDevice, s));
+    FPG_CUDA(cudaMemcpyAsync(m->staging + nodes, v, nodes * sizeof(float), cudaMemcpyHostToDevice, s));
+    FPG_CUDA(cudaMemcpyAsync(m->staging + 2 * nodes, w, nodes * sizeof(float), cudaMemcpyHostToDevice, s));
+    return met_pack(m, which, m->staging, m->staging + nodes, m->staging + 2 * nodes, s);
+}
+
+extern "C" fpg_status fpg_met_upload_frame_device(fpg_met* m, int32_t which, const float* u, const float* v,
+                                                  const float* w, void* stream) {
+    if (!m || !u || !v || !w || (which != 0 && which != 1)) return FPG_ERR_INVALID_ARGUMENT;
+    return met_pack(m, which, u, v, w, m->ctx->pick(stream));
+}
+
+extern "C" fpg_status fpg_met_set_level_heights(fpg_met* m, const float* heights, size_t n) {
+    if (!m || (!heights && n)) return FPG_ERR_INVALID_ARGUMENT;
+    if (n > FPG_MAX_LEVELS) return FPG_ERR_TOO_MANY_LEVELS;
+    if (n != m->nz) return FPG_ERR_LENGTH_MISMATCH;
+    std::memcpy(m->heights, heights, n * sizeof(float));
+    FPG_CUDA(cudaMemcpyAsync(m->heights_dev, m->heights, n * sizeof(float), cudaMemcpyHostToDevice, m->ctx->stream));
+    FPG_CUDA(cudaStreamSynchronize(m->ctx->stream));
+    m->monotonic = true;
+    for (size_t k = 1; k < n; ++k)
+        if (!(heights[k] >= heights[k - 1])) m->monotonic = false;
+    m->heights_set = true;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_pbl_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_pbl** out) {
+    if (!ctx || !out) return FPG_ERR_INVALID_ARGUMENT;
+    if (nx == 0 || ny == 0) return FPG_ERR_ZERO_SHAPE;
+    if (nx * ny >= (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    fpg_pbl* p = new fpg_pbl();
+    p->ctx = ctx; p->nx = nx; p->ny = ny;
+    const size_t n = nx * ny;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 7 && e == cudaSuccess; ++k) e = cudaMalloc(&p->field[k], n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->packed, n * sizeof(float4));
+    if (e != cudaSuccess) {
+        for (int k = 0; k < 7; ++k) cudaFree(p->field[k]);
+        cudaFree(p->packed);
+        delete p;
+        return cuda_status(e);
+    }
+    *out = p;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_pbl_destroy(fpg_pbl* p) {
+    if (!p) return FPG_OK;
+    for (int k = 0; k < 7; ++k) cudaFree(p->field[k]);
+    cudaFree(p->packed);
+    delete p;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_pbl_upload(fpg_pbl* p, const float* ustar, const float* wstar, const float* hmix,
+                                     const float* oli, const float* sshf, const float* ssr, const float* surfstr,
+                                     void* stream) {
+    if (!p || !ustar || !wstar || !hmix || !oli) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = p->ctx->pick(stream);
+    const size_t n = p->nx * p->ny;
+    const float* src[7] = {ustar, wstar, hmix, oli, sshf, ssr, surfstr};
+    for (int k = 0; k < 7; ++k) {
+        if (src[k]) FPG_CUDA(cudaMemcpyAsync(p->field[k], src[k], n * sizeof(float), cudaMemcpyHostToDevice, s));
+        else FPG_CUDA(cudaMemsetAsync(p->field[k], 0, n * sizeof(float), s));
+    }
+    pack_pbl_kernel<<<blocks_for(n, 256), 256, 0, s>>>(p->field[0], p->field[1], p->field[2], p->field[3],
+                                                        (uint32_t)n, p->packed);
+    p->ctx->count();
+    FPG_CHECK_LAUNCH();
+    p->ready = true;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_pbl_download(fpg_pbl* p, float* ustar, float* wstar, float* hmix, float* oli, float* sshf,
+                                       float* ssr, float* surfstr, void* stream) {
+    if (!p) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = p->ctx->pick(stream);
+    const size_t n = p->nx * p->ny;
+    float* dst[7] = {ustar, wstar, hmix, oli, sshf, ssr, surfstr};
+    for (int k = 0; k < 7; ++k)
+        if (dst[k]) FPG_CUDA(cudaMemcpyAsync(dst[k], p->field[k], n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    FPG_CUDA(cudaStreamSynchronize(s));
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_surface_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_surface** out) {
+    if (!ctx || !out) return FPG_ERR_INVALID_ARGUMENT;
+    if (nx == 0 || ny == 0) return FPG_ERR_ZERO_SHAPE;
+    if (nx * ny >= (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    fpg_surface* s = new fpg_surface();
+    s->ctx = ctx; s->nx = nx; s->ny = ny;
+    cudaError_t e = cudaMalloc(&s->frame[0], nx * ny * sizeof(fpg_surface_cell));
+    if (e == cudaSuccess) e = cudaMalloc(&s->frame[1], nx * ny * sizeof(fpg_surface_cell));
+    if (e != cudaSuccess) {
+        cudaFree(s->frame[0]); cudaFree(s->frame[1]); delete s;
+        return cuda_status(e);
+    }
+    *out = s;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_surface_destroy(fpg_surface* s) {
+    if (!s) return FPG_OK;
+    cudaFree(s->frame[0]);
+    cudaFree(s->frame[1]);
+    delete s;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_surface_upload(fpg_surface* s, int32_t which, const fpg_surface_cell* cells, void* stream) {
+    if (!s || !cells || (which != 0 && which != 1)) return FPG_ERR_INVALID_ARGUMENT;
+    FPG_CUDA(cudaMemcpyAsync(s->frame[which], cells, s->nx * s->ny * sizeof(fpg_surface_cell),
+                             cudaMemcpyHostToDevice, s->ctx->pick(stream)));
+    s->uploaded[which] = true;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_pbl_diagnostics(fpg_ctx* ctx, const fpg_surface* surface, float alpha,
+                                          const fpg_pbl_options* options, fpg_pbl* pbl, void* stream) {
+    if (!ctx || !surface || !options || !pbl) return FPG_ERR_INVALID_ARGUMENT;
+    if (surface->nx != pbl->nx || surface->ny != pbl->ny) return FPG_ERR_SHAPE_MISMATCH;
+    if (!surface->uploaded[0] || !surface->uploaded[1]) return FPG_ERR_NOT_READY;
+    cudaStream_t s = ctx->pick(stream);
+    const uint32_t n = (uint32_t)(pbl->nx * pbl->ny);
+    pbl_diag_kernel<<<blocks_for(n, 256), 256, 0, s>>>(surface->frame[0], surface->frame[1], alpha, *options, n,
+                                                        pbl->field[0], pbl->field[1], pbl->field[2], pbl->field[3],
+                                                        pbl->field[4], pbl->field[5], pbl->field[6], pbl->packed);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
+    pbl->ready = true;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_cellfield_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_cellfield** out) {
+    if (!ctx || !out) return FPG_ERR_INVALID_ARGUMENT;
+    if (nx == 0 || ny == 0) return FPG_ERR_ZERO_SHAPE;
+    if (nx * ny >= (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    fpg_cellfield* f = new fpg_cellfield();
+    f->ctx = ctx; f->nx = nx; f->ny = ny;
+    cudaError_t e = cudaMalloc(&f->lf, nx * ny * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMalloc(&f->staging, nx * ny * 3 * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaFree(f->lf); cudaFree(f->staging); delete f;
+        return cuda_status(e);
+    }
+    *out = f;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_cellfield_destroy(fpg_cellfield* f) {
+    if (!f) return FPG_OK;
+    cudaFree(f->lf);
+    cudaFree(f->staging);
+    delete f;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_cellfield_upload(fpg_cellfield* f, const float* lambda, const float* fraction,
+                                           void* stream) {
+    if (!f || !lambda || !fraction) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = f->ctx->pick(stream);
+    const size_t n = f->nx * f->ny;
+    // interleave on the device: (lambda, fraction) pairs
+    FPG_CUDA(cudaMemcpy2DAsync(f->lf, sizeof(float2), lambda, sizeof(float), sizeof(float), n,
+                               cudaMemcpyHostToDevice, s));
+    FPG_CUDA(cudaMemcpy2DAsync(reinterpret_cast<float*>(f->lf) + 1, sizeof(float2), fraction, sizeof(float),
+                               sizeof(float), n, cudaMemcpyHostToDevice, s));
+    f->ready = true;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_cellfield_from_precipitation(fpg_cellfield* f, const float* lsp, const float* convp,
+                                                       const float* cloud_cover, float a, float b, void* stream) {
+    if (!f) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = f->ctx->pick(stream);
+    const size_t n = f->nx * f->ny;
+    float* d_lsp = f->staging;
+    float* d_conv = f->staging + n;
+    float* d_cc = f->staging + 2 * n;
+    if (lsp) FPG_CUDA(cudaMemcpyAsync(d_lsp, lsp, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    else FPG_CUDA(cudaMemsetAsync(d_lsp, 0, n * sizeof(float), s));
+    if (convp) FPG_CUDA(cudaMemcpyAsync(d_conv, convp, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    else FPG_CUDA(cudaMemsetAsync(d_conv, 0, n * sizeof(float), s));
+    if (cloud_cover) {
+        FPG_CUDA(cudaMemcpyAsync(d_cc, cloud_cover, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    } else {
+        fill_kernel<<<blocks_for(n, 256), 256, 0, s>>>(d_cc, (uint32_t)n, 1.0f);  // cloud cover 1
+        f->ctx->count();
+        FPG_CHECK_LAUNCH();
+    }
+    wet_cells_kernel<<<blocks_for(n, 256), 256, 0, s>>>(d_lsp, d_conv, d_cc, a, b, (uint32_t)n, f->lf);
+    f->ctx->count();
+    FPG_CHECK_LAUNCH();
+    f->ready = true;
+    return FPG_OK;
+}
+
+// ============================================================================
+// C ABI: the step
+// ============================================================================
+
+extern "C" void fpg_step_params_default(fpg_step_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->stages = FPG_STAGE_ALL;
+    p->alpha = 0.0f;
+    p->dt_seconds = 1.0f;
+    p->turb_dt_seconds = 1.0f;
+    p->x_grid_per_meter = 1.0f;
+    p->y_grid_per_meter = 1.0f;
+    p->z_grid_per_meter = 1.0f;
+    p->n_substeps = 4;
+    p->min_height_m = 0.01f;
+    p->dry_reference_height_m = 15.0f;
+    p->dry_mode = FPG_FORCING_NONE;
+    p->wet_mode = FPG_FORCING_NONE;
+}
+
+static void counter_add64(const uint32_t in[4], uint64_t off, uint32_t out[4]) {
+    // philox_counter_add (rng.rs:69-87)
+    const uint32_t lo = (uint32_t)off, hi = (uint32_t)(off >> 32);
+    uint32_t c0 = in[0] + lo;
+    uint32_t carry0 = c0 < in[0];
+    uint32_t n1 = in[1] + hi;
+    uint32_t carry1a = n1 < in[1];
+    uint32_t c1 = n1 + carry0;
+    uint32_t carry1b = c1 < n1;
+    uint32_t c2 = in[2] + (carry1a | carry1b);
+    uint32_t carry2 = c2 < in[2];
+    uint32_t c3 = in[3] + carry2;
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+extern "C" fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* P, const fpg_met* met, const fpg_pbl* pbl,
+                               const fpg_step_params* prm, uint32_t next_counter[4], void* stream) {
+    if (!ctx || !P || !prm) return FPG_ERR_INVALID_ARGUMENT;
+    if (next_counter) std::memcpy(next_counter, prm->counter, sizeof(uint32_t) * 4);
+    const size_t n = P->dispatch;
+    if (n == 0) return FPG_OK;                          // empty set: Ok, counter unchanged
+    if (n > (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    const uint32_t st = prm->stages & FPG_STAGE_ALL;
+    const bool adv = st & FPG_STAGE_ADVECT, turb = st & FPG_STAGE_TURBULENCE;
+    const bool dry = (st & FPG_STAGE_DRY) && prm->dry_mode != FPG_FORCING_NONE;
+    const bool wet = (st & FPG_STAGE_WET) && prm->wet_mode != FPG_FORCING_NONE;
+    if (adv) {
+        if (!met) return FPG_ERR_INVALID_ARGUMENT;
+        if (!met->uploaded[0] || !met->uploaded[1]) return FPG_ERR_NOT_READY;
+        if (!std::isfinite(prm->dt_seconds)) return FPG_ERR_INVALID_TIME_STEP;   // gpu/advection.rs:618
+    }
+    if (turb) {
+        if (!pbl) return FPG_ERR_INVALID_ARGUMENT;
+        if (!pbl->ready) return FPG_ERR_NOT_READY;
+        if (!std::isfinite(prm->turb_dt_seconds) || prm->turb_dt_seconds <= 0.0f)
+            return FPG_ERR_INVALID_TIME_STEP;                                      // langevin_fused.rs:147
+    }
+    if (dry) {
+        if (prm->dry_mode < FPG_FORCING_UNIFORM || prm->dry_mode > FPG_FORCING_PER_PARTICLE)
+            return FPG_ERR_INVALID_ARGUMENT;
+        if (prm->dry_mode == FPG_FORCING_PER_PARTICLE && !prm->dry_velocity_dev) return FPG_ERR_INVALID_ARGUMENT;
+        if (!std::isfinite(prm->turb_dt_seconds)) return FPG_ERR_INVALID_TIME_STEP;  // deposition.rs:334
+        if (!std::isfinite(prm->dry_reference_height_m) || prm->dry_reference_height_m <= 0.0f)
+            return FPG_ERR_INVALID_REFERENCE_HEIGHT;                                 // deposition.rs:339
+    }
+    if (wet) {
+        if (prm->wet_mode < FPG_FORCING_UNIFORM || prm->wet_mode > FPG_FORCING_PER_CELL)
+            return FPG_ERR_INVALID_ARGUMENT;
+        if (prm->wet_mode == FPG_FORCING_PER_PARTICLE && (!prm->wet_lambda_dev || !prm->wet_fraction_dev))
+            return FPG_ERR_INVALID_ARGUMENT;
+        if (prm->wet_mode == FPG_FORCING_PER_CELL && (!prm->wet_cells || !prm->wet_cells->ready))
+            return FPG_ERR_NOT_READY;
+        if (!std::isfinite(prm->turb_dt_seconds)) return FPG_ERR_INVALID_TIME_STEP;  // wet_deposition.rs:387
+    }
+
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.cell_x = (int32_t*)P->field[FPG_FIELD_CELL_X];
+    a.cell_y = (int32_t*)P->field[FPG_FIELD_CELL_Y];
+    a.pos_x = (float*)P->field[FPG_FIELD_POS_X];
+    a.pos_y = (float*)P->field[FPG_FIELD_POS_Y];
+    a.pos_z = (float*)P->field[FPG_FIELD_POS_Z];
+    a.flags = (const uint32_t*)P->field[FPG_FIELD_FLAGS];
+    for (int k = 0; k < 4; ++k) a.mass[k] = (float*)P->field[FPG_FIELD_MASS0 + k];
+    a.vel_u = (float*)P->field[FPG_FIELD_VEL_U];
+    a.vel_v = (float*)P->field[FPG_FIELD_VEL_V];
+    a.vel_w = (float*)P->field[FPG_FIELD_VEL_W];
+    a.turb_u = (float*)P->field[FPG_FIELD_TURB_U];
+    a.turb_v = (float*)P->field[FPG_FIELD_TURB_V];
+    a.turb_w = (float*)P->field[FPG_FIELD_TURB_W];
+    a.cbt = (int32_t*)P->field[FPG_FIELD_CBT];
+    a.n = (uint32_t)n;
+    a.n_species = P->n_species;
+    a.stages = (adv ? FPG_STAGE_ADVECT : 0u) | (turb ? FPG_STAGE_TURBULENCE : 0u) | (dry ? FPG_STAGE_DRY : 0u) |
+               (wet ? FPG_STAGE_WET : 0u);
+    size_t smem = 0;
+    if (adv) {
+        a.bracket = met->bracket;
+        a.nx = (uint32_t)met->nx; a.ny = (uint32_t)met->ny; a.nz = (uint32_t)met->nz;
+        a.has_heights = met->heights_set && met->heights[met->nz - 1] > 0.0f;
+        a.monotonic = met->monotonic;
+        // gpu/advection.rs:639: alpha clamped to [0, 1]
+        a.alpha = fminf(fmaxf(prm->alpha, 0.0f), 1.0f);
+        a.dt = prm->dt_seconds;
+        a.xs = prm->x_grid_per_meter; a.ys = prm->y_grid_per_meter; a.zs = prm->z_grid_per_meter;
+        smem = met->nz * sizeof(float);
+        a.heights = met->heights_dev;
+    }
+    if (turb) {
+        a.pbl = pbl->packed;
+        a.pnx = (uint32_t)pbl->nx; a.pny = (uint32_t)pbl->ny;
+        a.tdt = prm->turb_dt_seconds;
+        a.rho = prm->rho_grad_over_rho;
+        a.zmin = prm->min_height_m;
+        a.n_sub = prm->n_substeps;
+        a.key0 = prm->key[0]; a.key1 = prm->key[1];
+        a.counter = u32x4{prm->counter[0], prm->counter[1], prm->counter[2], prm->counter[3]};
+    } else {
+        a.tdt = prm->turb_dt_seconds;
+    }
+    a.href = fmaxf(prm->dry_reference_height_m, 0.1f);                // dry_deposition.wgsl:89
+    a.dry_mode = dry ? prm->dry_mode : FPG_FORCING_NONE;
+    a.dry_v = prm->dry_velocity_m_s;
+    a.dry_v_arr = prm->dry_velocity_dev;
+    a.dry_prob = prm->dry_probability_dev;
+    a.wet_mode = wet ? prm->wet_mode : FPG_FORCING_NONE;
+    a.wet_l = prm->wet_lambda_s_inv;
+    a.wet_f = prm->wet_fraction;
+    a.wet_l_arr = prm->wet_lambda_dev;
+    a.wet_f_arr = prm->wet_fraction_dev;
+    if (wet && prm->wet_mode == FPG_FORCING_PER_CELL) {
+        a.wet_cells = prm->wet_cells->lf;
+        a.wnx = (uint32_t)prm->wet_cells->nx; a.wny = (uint32_t)prm->wet_cells->ny;
+    }
+    a.wet_prob = prm->wet_probability_dev;
+
+    cudaStream_t s = ctx->pick(stream);
+    fused_step_kernel<<<blocks_for(n, 256), 256, smem, s>>>(a);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
+    if (turb && next_counter) {
+        // gpu/langevin_fused.rs:229-233
+        const uint64_t bpp = prm->n_substeps <= 2u ? 1u : 2u;
+        counter_add64(prm->counter, (uint64_t)n * bpp, next_counter);
+    }
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_advect_dual_wind(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met, float alpha,
+                                           float dt_seconds, float xs, float ys, float zs, void* stream) {
+    fpg_step_params p;
+    fpg_step_params_default(&p);
+    p.stages = FPG_STAGE_ADVECT;
+    p.alpha = alpha;
+    p.dt_seconds = dt_seconds;
+    p.x_grid_per_meter = xs; p.y_grid_per_meter = ys; p.z_grid_per_meter = zs;
+    return fpg_step(ctx, particles, met, nullptr, &p, nullptr, stream);
+}
+
+extern "C" fpg_status fpg_langevin_fused(fpg_ctx* ctx, fpg_particles* particles, const fpg_pbl* pbl, float dt,
+                                         float rho_grad_over_rho, uint32_t n_substeps, float min_height_m,
+                                         const uint32_t key[2], const uint32_t base_counter[4],
+                                         uint32_t next_counter[4], void* stream) {
+    if (!key || !base_counter) return FPG_ERR_INVALID_ARGUMENT;
+    fpg_step_params p;
+    fpg_step_params_default(&p);
+    p.stages = FPG_STAGE_TURBULENCE;
+    p.turb_dt_seconds = dt;
+    p.rho_grad_over_rho = rho_grad_over_rho;
+    p.n_substeps = n_substeps;
+    p.min_height_m = min_height_m;
+    p.key[0] = key[0]; p.key[1] = key[1];
+    std::memcpy(p.counter, base_counter, sizeof(p.counter));
+    return fpg_step(ctx, particles, nullptr, pbl, &p, next_counter, stream);
+}
+
+extern "C" fpg_status fpg_dry_deposition(fpg_ctx* ctx, fpg_particles* particles, const float* vdep_dev, float dt,
+                                         float href, float* prob_dev, void* stream) {
+    if (!vdep_dev) return FPG_ERR_INVALID_ARGUMENT;
+    fpg_step_params p;
+    fpg_step_params_default(&p);
+    p.stages = FPG_STAGE_DRY;
+    p.turb_dt_seconds = dt;
+    p.dry_reference_height_m = href;
+    p.dry_mode = FPG_FORCING_PER_PARTICLE;
+    p.dry_velocity_dev = vdep_dev;
+    p.dry_probability_dev = prob_dev;
+    return fpg_step(ctx, particles, nullptr, nullptr, &p, nullptr, stream);
+}
+
+extern "C" fpg_status fpg_wet_deposition(fpg_ctx* ctx, fpg_particles* particles, const float* lambda_dev,
+                                         const float* fraction_dev, float dt, float* prob_dev, void* stream) {
+    if (!lambda_dev || !fraction_dev) return FPG_ERR_INVALID_ARGUMENT;
+    fpg_step_params p;
+    fpg_step_params_default(&p);
+    p.stages = FPG_STAGE_WET;
+    p.turb_dt_seconds = dt;
+    p.wet_mode = FPG_FORCING_PER_PARTICLE;
+    p.wet_lambda_dev = lambda_dev;
+    p.wet_fraction_dev = fraction_dev;
+    p.wet_probability_dev = prob_dev;
+    return fpg_step(ctx, particles, nullptr, nullptr, &p, nullptr, stream);
+}
+
+extern "C" fpg_status fpg_philox_uniforms(fpg_ctx* ctx, const uint32_t key[2], const uint32_t counter[4],
+                                          size_t n_blocks, float* out_dev, uint32_t* raw_dev, void* stream) {
+    if (!ctx || !key || !counter) return FPG_ERR_INVALID_ARGUMENT;
+    if (n_blocks == 0) return FPG_OK;
+    if (n_blocks > (size_t)UINT32_MAX / 4) return FPG_ERR_VALUE_TOO_LARGE;
+    cudaStream_t s = ctx->pick(stream);
+    philox_kernel<<<blocks_for(n_blocks, 256), 256, 0, s>>>(key[0], key[1],
+                                                             u32x4{counter[0], counter[1], counter[2], counter[3]},
+                                                             (uint32_t)n_blocks, out_dev, raw_dev);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
+    return FPG_OK;
+}

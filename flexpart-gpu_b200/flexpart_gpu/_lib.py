@@ -1,0 +1,134 @@
+"""ctypes binding of libfpg.so (include/fpg.h).
+
+The library is the only compute path: importing this module raises if the
+built library is missing, and nothing here falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .records import PblOptions, StepParams
+
+_PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.environ.get("FPG_LIBRARY", os.path.join(_PKG_ROOT, "lib", "libfpg.so"))
+
+
+class FpgError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        msg = lib.fpg_status_string(status).decode() if lib is not None else str(status)
+        extra = ""
+        if status == -100:
+            extra = f" (cudaError {lib.fpg_last_cuda_error()})"
+        super().__init__(f"{what}: {msg} [{status}]{extra}")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libfpg.so not found at {LIB_PATH}; build it with `make -C flexpart-gpu_b200` "
+            "(there is no CPU fallback)")
+    return ctypes.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+_i32 = ctypes.c_int32
+_u32 = ctypes.c_uint32
+_f32 = ctypes.c_float
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+def _sig(name, restype, *argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_sig("fpg_status_string", ctypes.c_char_p, _i32)
+_sig("fpg_last_cuda_error", _i32)
+_sig("fpg_abi_version", _i32)
+_sig("fpg_ctx_create", _i32, _i32, ctypes.POINTER(_vp))
+_sig("fpg_ctx_destroy", _i32, _vp)
+_sig("fpg_ctx_stream", _vp, _vp)
+_sig("fpg_ctx_synchronize", _i32, _vp, _vp)
+_sig("fpg_ctx_kernel_launches", ctypes.c_uint64, _vp)
+_sig("fpg_device_alloc", _i32, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_device_free", _i32, _vp, _vp)
+_sig("fpg_memcpy", _i32, _vp, _vp, _vp, _sz, _i32, _vp)
+_sig("fpg_memset", _i32, _vp, _vp, _i32, _sz, _vp)
+_sig("fpg_particles_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_particles_destroy", _i32, _vp)
+_sig("fpg_particles_capacity", _sz, _vp)
+_sig("fpg_particles_dispatch_count", _sz, _vp)
+_sig("fpg_particles_set_dispatch_count", _i32, _vp, _sz)
+_sig("fpg_particles_upload", _i32, _vp, _sz, _sz, _vp, _vp)
+_sig("fpg_particles_upload_slots", _i32, _vp, _vp, _sz, _vp, _vp)
+_sig("fpg_particles_download", _i32, _vp, _sz, _sz, _vp, _vp)
+_sig("fpg_particles_field", _vp, _vp, _i32)
+_sig("fpg_particles_copy_field", _i32, _vp, _i32, _sz, _sz, _vp, _i32, _vp)
+_sig("fpg_met_create", _i32, _vp, _sz, _sz, _sz, ctypes.POINTER(_vp))
+_sig("fpg_met_destroy", _i32, _vp)
+_sig("fpg_met_upload_frame", _i32, _vp, _i32, _vp, _vp, _vp, _vp)
+_sig("fpg_met_upload_frame_device", _i32, _vp, _i32, _vp, _vp, _vp, _vp)
+_sig("fpg_met_set_level_heights", _i32, _vp, _vp, _sz)
+_sig("fpg_pbl_create", _i32, _vp, _sz, _sz, ctypes.POINTER(_vp))
+_sig("fpg_pbl_destroy", _i32, _vp)
+_sig("fpg_pbl_upload", _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_pbl_download", _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_surface_create", _i32, _vp, _sz, _sz, ctypes.POINTER(_vp))
+_sig("fpg_surface_destroy", _i32, _vp)
+_sig("fpg_surface_upload", _i32, _vp, _i32, _vp, _vp)
+_sig("fpg_pbl_diagnostics", _i32, _vp, _vp, _f32, ctypes.POINTER(PblOptions), _vp, _vp)
+_sig("fpg_cellfield_create", _i32, _vp, _sz, _sz, ctypes.POINTER(_vp))
+_sig("fpg_cellfield_destroy", _i32, _vp)
+_sig("fpg_cellfield_upload", _i32, _vp, _vp, _vp, _vp)
+_sig("fpg_cellfield_from_precipitation", _i32, _vp, _vp, _vp, _vp, _f32, _f32, _vp)
+_sig("fpg_step_params_default", None, ctypes.POINTER(StepParams))
+_sig("fpg_step", _i32, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams), _u32p, _vp)
+_sig("fpg_advect_dual_wind", _i32, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _f32, _vp)
+_sig("fpg_langevin_fused", _i32, _vp, _vp, _vp, _f32, _f32, _u32, _f32, _u32p, _u32p, _u32p, _vp)
+_sig("fpg_dry_deposition", _i32, _vp, _vp, _vp, _f32, _f32, _vp, _vp)
+_sig("fpg_wet_deposition", _i32, _vp, _vp, _vp, _vp, _f32, _vp, _vp)
+_sig("fpg_grid_create", _i32, _vp, _sz, _sz, _sz, ctypes.POINTER(_vp))
+_sig("fpg_grid_destroy", _i32, _vp)
+_sig("fpg_grid_accumulate", _i32, _vp, _vp, _vp, _u32, _f32, _vp, _sz, _vp)
+_sig("fpg_grid_cell_indices", _i32, _vp, _vp, _vp, _vp, _sz, _vp, _vp)
+_sig("fpg_grid_download", _i32, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_grid_counts_device", _vp, _vp)
+_sig("fpg_grid_mass_device", _vp, _vp)
+_sig("fpg_compaction_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_compaction_destroy", _i32, _vp)
+_sig("fpg_compact", _i32, _vp, _vp, _vp, _u32p, _vp, _vp)
+_sig("fpg_philox_uniforms", _i32, _vp, _u32p, _u32p, _sz, _vp, _vp, _vp)
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise FpgError(status, what)
+
+
+# Every symbol include/fpg.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "fpg_status_string", "fpg_last_cuda_error", "fpg_abi_version",
+    "fpg_ctx_create", "fpg_ctx_destroy", "fpg_ctx_stream", "fpg_ctx_synchronize", "fpg_ctx_kernel_launches",
+    "fpg_device_alloc", "fpg_device_free", "fpg_memcpy", "fpg_memset",
+    "fpg_particles_create", "fpg_particles_destroy", "fpg_particles_capacity", "fpg_particles_dispatch_count",
+    "fpg_particles_set_dispatch_count", "fpg_particles_upload", "fpg_particles_upload_slots",
+    "fpg_particles_download", "fpg_particles_field", "fpg_particles_copy_field",
+    "fpg_met_create", "fpg_met_destroy", "fpg_met_upload_frame", "fpg_met_upload_frame_device",
+    "fpg_met_set_level_heights",
+    "fpg_pbl_create", "fpg_pbl_destroy", "fpg_pbl_upload", "fpg_pbl_download",
+    "fpg_surface_create", "fpg_surface_destroy", "fpg_surface_upload", "fpg_pbl_diagnostics",
+    "fpg_cellfield_create", "fpg_cellfield_destroy", "fpg_cellfield_upload", "fpg_cellfield_from_precipitation",
+    "fpg_step_params_default", "fpg_step", "fpg_advect_dual_wind", "fpg_langevin_fused",
+    "fpg_dry_deposition", "fpg_wet_deposition",
+    "fpg_grid_create", "fpg_grid_destroy", "fpg_grid_accumulate", "fpg_grid_cell_indices", "fpg_grid_download",
+    "fpg_grid_counts_device", "fpg_grid_mass_device",
+    "fpg_compaction_create", "fpg_compaction_destroy", "fpg_compact",
+    "fpg_philox_uniforms",
+]

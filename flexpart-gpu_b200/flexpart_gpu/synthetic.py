@@ -1,0 +1,230 @@
+"""Seeded synthetic inputs of the benchmark configurations.
+
+No public dataset is involved: the meteorology, sources and surface fields
+are drawn from the value distributions the configurations state
+(u, v ~ N(5, 3) m/s smoothed by a Gaussian filter of sigma 3 cells and
+renormalised to those moments, w ~ N(0, 0.05) m/s, PBL height U(300, 1500) m,
+u* U(0.1, 0.6) m/s, 1/L ~ N(0, 0.01) 1/m, temperature from a 6.5 K/km lapse
+rate, precipitation lognormal(-1, 1) mm/h on 30 % of cells), with a fixed
+numpy seed per configuration, so every run and every process sees the same
+arrays.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .records import PARTICLE_DTYPE, SURFACE_DTYPE
+
+R_EARTH = 6_371_000.0  # src/bin/fortran-validation.rs:21
+
+
+@dataclass
+class MetSpec:
+    nx: int
+    ny: int
+    nz: int
+    dx_deg: float
+    dy_deg: float
+    xlon0: float
+    ylat0: float
+    top_m: float = 15_000.0
+    n_frames: int = 2
+    frame_seconds: int = 3 * 3600
+    seed: int = 0
+    wet: bool = False
+
+
+@dataclass
+class Source:
+    lon: float
+    lat: float
+    z_min: float
+    z_max: float
+    mass_kg: float
+    particle_count: int
+    start: int  # seconds since epoch
+    end: int
+    lon_max: float | None = None
+    lat_max: float | None = None
+
+
+@dataclass
+class Scenario:
+    name: str
+    met: MetSpec
+    sources: list
+    start: int
+    end: int
+    dt: int
+    out_shape: tuple
+    outheights: list
+    key: tuple = (42, 0)
+    dry_velocity: float = 0.002
+    wet_a: float = 1.0e-4
+    wet_b: float = 0.8
+    capacity: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n_steps(self) -> int:
+        # has_remaining_steps is inclusive (simulation/timeloop.rs:832-834)
+        return (self.end - self.start) // self.dt + 1
+
+
+def level_heights(nz: int, top_m: float) -> np.ndarray:
+    """Terrain-following levels stretched quadratically to `top_m` (no terrain:
+    heights are the same in every column)."""
+    k = np.arange(1, nz + 1, dtype=np.float64)
+    return (top_m * (k / nz) ** 2).astype(np.float32)
+
+
+def velocity_scale(spec: MetSpec) -> tuple:
+    """One global metres->grid factor at the domain-centre latitude
+    (VelocityToGridScale, src/physics/advection.rs:36-41, built as in
+    src/bin/fortran-validation.rs:123-138)."""
+    lat_c = spec.ylat0 + 0.5 * (spec.ny - 1) * spec.dy_deg
+    dx_m = R_EARTH * math.cos(math.radians(lat_c)) * math.radians(spec.dx_deg)
+    dy_m = R_EARTH * math.radians(spec.dy_deg)
+    return (float(np.float32(1.0 / dx_m)), float(np.float32(1.0 / dy_m)), 1.0)
+
+
+def _smooth_normal(rng, shape, mean, std, sigma_cells):
+    from scipy.ndimage import gaussian_filter
+
+    a = rng.standard_normal(shape)
+    a = gaussian_filter(a, sigma=(sigma_cells, sigma_cells, 0), mode="wrap")
+    a = (a - a.mean()) / max(a.std(), 1e-12)
+    return (mean + std * a).astype(np.float32)
+
+
+def make_frames(spec: MetSpec):
+    """Returns a list of n_frames dicts with u, v, w of shape (nx, ny, nz)
+    in the reference layout ((ix*ny)+iy)*nz+iz, and the surface cell
+    records of each frame."""
+    rng = np.random.default_rng(1_000 + spec.seed)
+    shape = (spec.nx, spec.ny, spec.nz)
+    pbl_h = rng.uniform(300.0, 1500.0, (spec.nx, spec.ny)).astype(np.float32)
+    ustar = rng.uniform(0.1, 0.6, (spec.nx, spec.ny)).astype(np.float32)
+    oli = rng.normal(0.0, 0.01, (spec.nx, spec.ny)).astype(np.float32)
+    frames = []
+    for f in range(spec.n_frames):
+        u = _smooth_normal(rng, shape, 5.0, 3.0, 3.0)
+        v = _smooth_normal(rng, shape, 5.0, 3.0, 3.0)
+        w = rng.normal(0.0, 0.05, shape).astype(np.float32)
+        # PBL inputs vary slowly between frames (+-10 %)
+        h_f = (pbl_h * rng.uniform(0.9, 1.1, pbl_h.shape)).astype(np.float32)
+        us_f = (ustar * rng.uniform(0.9, 1.1, ustar.shape)).astype(np.float32)
+        oli_f = (oli * rng.uniform(0.9, 1.1, oli.shape)).astype(np.float32)
+        frames.append({"u": u, "v": v, "w": w, "surface": surface_cells(spec, u, v, h_f, us_f, oli_f)})
+    return frames
+
+
+def surface_cells(spec: MetSpec, u, v, hmix, ustar, oli) -> np.ndarray:
+    """fpg_surface_cell records with met-provided u*, 1/L and h, and the
+    sensible heat flux that gives the same L through the flux formula
+    (pbl_diagnostics.wgsl:168-195: L = -(rho cp T u*^3) / (kappa g H))."""
+    n = spec.nx * spec.ny
+    cells = np.zeros(n, SURFACE_DTYPE)
+    t2m = np.float32(288.15)                     # sea level; 6.5 K/km lapse aloft
+    sp = np.float32(101_325.0)
+    rho = sp / (np.float32(287.05) * t2m)
+    cells["surface_pressure_pa"] = sp
+    cells["temperature_2m_k"] = t2m
+    cells["u10_ms"] = u[:, :, 0].reshape(n)
+    cells["v10_ms"] = v[:, :, 0].reshape(n)
+    us = ustar.reshape(n).astype(np.float32)
+    cells["surface_stress_n_m2"] = (rho * us * us).astype(np.float32)
+    shf = -(rho * np.float32(1004.6) * t2m * us ** 3) * oli.reshape(n) / (np.float32(0.4) * np.float32(9.81))
+    cells["sensible_heat_flux_w_m2"] = shf.astype(np.float32)
+    cells["solar_radiation_w_m2"] = np.float32(250.0)
+    cells["mixing_height_m"] = hmix.reshape(n)
+    cells["friction_velocity_ms"] = us
+    cells["inv_obukhov_length_per_m"] = oli.reshape(n)
+    return cells
+
+
+def precipitation(spec: MetSpec, frame: int):
+    """Lognormal(-1, 1) mm/h on a random 30 % of cells (large-scale), zero
+    elsewhere; no convective part; cloud cover 1."""
+    rng = np.random.default_rng(5_000 + 31 * spec.seed + frame)
+    n = spec.nx * spec.ny
+    lsp = np.zeros(n, np.float32)
+    on = rng.random(n) < 0.30
+    lsp[on] = rng.lognormal(-1.0, 1.0, int(on.sum())).astype(np.float32)
+    return lsp
+
+
+EPOCH_2024 = 1_704_067_200  # 2024-01-01 00:00:00 UTC
+
+
+def config0() -> Scenario:
+    """100 k particles, one point release of 1 kg spread over 1 h at 50 m AGL;
+    met 90x60 (0.5 deg) x 20 levels to 15 km; 2 frames 3 h apart cycled for
+    24 h; dt 900 s (97 inclusive steps); output 90x60x3 (100, 500, 1000 m)."""
+    met = MetSpec(nx=90, ny=60, nz=20, dx_deg=0.5, dy_deg=0.5, xlon0=-10.0, ylat0=35.0, n_frames=2, seed=0)
+    t0 = EPOCH_2024
+    src = Source(lon=met.xlon0 + 15.25, lat=met.ylat0 + 15.25, z_min=50.0, z_max=50.0, mass_kg=1.0,
+                 particle_count=100_000, start=t0, end=t0 + 3600)
+    return Scenario("config0", met, [src], start=t0, end=t0 + 24 * 3600, dt=900, out_shape=(90, 60, 3),
+                    outheights=[100.0, 500.0, 1000.0], capacity=100_000)
+
+
+def config1(particles: int = 10_000_000) -> Scenario:
+    """10 M particles from 8 point sources (random locations, heights
+    U(10, 300) m, 1 kg/h each) released over 48 h; met 360x180 (1 deg) x 60
+    levels, 9 frames 3 h apart (cycled); wet scavenging on; output 360x180x5."""
+    met = MetSpec(nx=360, ny=180, nz=60, dx_deg=1.0, dy_deg=1.0, xlon0=-180.0, ylat0=-89.5, n_frames=9, seed=1,
+                  wet=True)
+    rng = np.random.default_rng(77)
+    t0 = EPOCH_2024
+    per = particles // 8
+    sources = []
+    for s in range(8):
+        lon = float(rng.uniform(-150.0, 150.0))
+        lat = float(rng.uniform(-60.0, 60.0))
+        z = float(rng.uniform(10.0, 300.0))
+        sources.append(Source(lon=lon, lat=lat, z_min=z, z_max=z, mass_kg=48.0,
+                              particle_count=per + (1 if s < particles - 8 * per else 0),
+                              start=t0, end=t0 + 48 * 3600))
+    return Scenario("config1", met, sources, start=t0, end=t0 + 48 * 3600, dt=900, out_shape=(360, 180, 5),
+                    outheights=[100.0, 500.0, 1000.0, 2000.0, 5000.0], capacity=particles)
+
+
+def bracket_frames(scn: Scenario, t: int):
+    """(frame index t0, frame index t1, time t0, time t1) of the bracket that
+    holds t; frames cycle with period n_frames."""
+    fs = scn.met.frame_seconds
+    k = (t - scn.start) // fs
+    if t - scn.start == k * fs and k > 0:
+        k -= 1  # at a frame time, stay in the bracket that ends there
+    ta = scn.start + k * fs
+    n = scn.met.n_frames
+    return int(k % n), int((k + 1) % n), ta, ta + fs
+
+
+def particles_at_sources(scn: Scenario, n: int, seed: int = 3) -> np.ndarray:
+    """n active particle records scattered in the boxes around the sources
+    (used where a test needs an already-spread population)."""
+    rng = np.random.default_rng(seed)
+    spec = scn.met
+    rec = np.zeros(n, PARTICLE_DTYPE)
+    src_idx = rng.integers(0, len(scn.sources), n)
+    lon = np.array([s.lon for s in scn.sources])[src_idx] + rng.normal(0, 3.0 * spec.dx_deg, n)
+    lat = np.array([s.lat for s in scn.sources])[src_idx] + rng.normal(0, 3.0 * spec.dy_deg, n)
+    x = np.clip((lon - spec.xlon0) / spec.dx_deg, 0, spec.nx - 1.001)
+    y = np.clip((lat - spec.ylat0) / spec.dy_deg, 0, spec.ny - 1.001)
+    fx, fy = np.floor(x), np.floor(y)
+    rec["cell_x"] = fx.astype(np.int32)
+    rec["cell_y"] = fy.astype(np.int32)
+    rec["pos_x"] = (x - fx).astype(np.float32)
+    rec["pos_y"] = (y - fy).astype(np.float32)
+    rec["pos_z"] = rng.uniform(1.0, 2500.0, n).astype(np.float32)
+    rec["flags"] = 1
+    rec["mass"][:, 0] = np.float32(1.0 / n)
+    rec["turb_u"] = rng.normal(0, 0.5, n).astype(np.float32)
+    rec["turb_v"] = rng.normal(0, 0.5, n).astype(np.float32)
+    rec["turb_w"] = rng.normal(0, 0.3, n).astype(np.float32)
+    return rec

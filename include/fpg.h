@@ -134,6 +134,16 @@ fpg_status fpg_ctx_synchronize(fpg_ctx* ctx, void* stream);
  * points, graph replays counted per kernel node). */
 uint64_t fpg_ctx_kernel_launches(fpg_ctx* ctx);
 
+/* Plain device buffers for callers without a CUDA allocator of their own
+ * (the role wgpu::Buffer plays for the reference's per-slot forcing and
+ * probability arrays, gpu/deposition.rs, gpu/wet_deposition.rs).
+ * fpg_memcpy kind: 0 host->device, 1 device->host (returns after the copy),
+ * 2 device->device. */
+fpg_status fpg_device_alloc(fpg_ctx* ctx, size_t bytes, void** out);
+fpg_status fpg_device_free(fpg_ctx* ctx, void* ptr);
+fpg_status fpg_memcpy(fpg_ctx* ctx, void* dst, const void* src, size_t bytes, int32_t kind, void* stream);
+fpg_status fpg_memset(fpg_ctx* ctx, void* dst, int32_t value, size_t bytes, void* stream);
+
 /* ------------------------------------------------------------------------
  * Particles (ParticleBuffers, src/gpu/buffers.rs:377-510)
  * ---------------------------------------------------------------------- */
@@ -350,6 +360,12 @@ fpg_status fpg_grid_destroy(fpg_grid* g);
 fpg_status fpg_grid_accumulate(fpg_ctx* ctx, const fpg_particles* particles, fpg_grid* grid,
                                uint32_t species_index, float mass_scale,
                                const float* outheights, size_t n_outheights, void* stream);
+/* Cell index ((ix*ny)+iy)*nz+iz that fpg_grid_accumulate would use for each
+ * slot [0, dispatch_count), 0xFFFFFFFF for inactive slots (the binning of
+ * concentration_gridding.wgsl:332-336 on its own).  out_dev: device array. */
+fpg_status fpg_grid_cell_indices(fpg_ctx* ctx, const fpg_particles* particles, const fpg_grid* grid,
+                                 const float* outheights, size_t n_outheights, uint32_t* out_dev,
+                                 void* stream);
 /* download_output (gridding.rs:191-219): counts, raw scaled masses and kg
  * (= scaled / mass_scale as f32); any pointer may be NULL. */
 fpg_status fpg_grid_download(fpg_grid* g, uint32_t* counts, uint32_t* mass_scaled, float* mass_kg,

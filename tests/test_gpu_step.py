@@ -1,0 +1,248 @@
+"""GPU parity of the fused step and its seam functions against the oracle.
+
+Every call goes through the C ABI (libfpg.so via ctypes).  Tolerance: the
+floating-point fields agree to relative 1e-5 (absolute 1e-5 below 1) after
+one step; integer fields (cells, flags, cbt) and Philox outputs are
+bit-exact.  The error of both against the FP64 oracle is printed.
+"""
+import numpy as np
+import pytest
+
+from helpers import REL_TOL, close, oracle_step, pbl_arrays, population, production_params, small_met
+from oracle import orc
+
+pytestmark = pytest.mark.gpu
+
+api = pytest.importorskip("flexpart_gpu.api")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def _gpu_setup(ctx, spec, frames, met, alpha, rec):
+    m = api.Met(ctx, spec.nx, spec.ny, spec.nz)
+    m.upload_frame(0, met["u0"], met["v0"], met["w0"])
+    m.upload_frame(1, met["u1"], met["v1"], met["w1"])
+    m.set_level_heights(met["heights"])
+    surf = api.Surface(ctx, spec.nx, spec.ny)
+    surf.upload(0, frames[0]["surface"])
+    surf.upload(1, frames[1]["surface"])
+    pbl = api.Pbl(ctx, spec.nx, spec.ny)
+    api.pbl_diagnostics(ctx, surf, alpha, pbl)
+    p = api.Particles(ctx, len(rec))
+    p.upload(rec)
+    return m, surf, pbl, p
+
+
+def _compare_state(g, s, label):
+    gx = g["cell_x"].astype(np.float64) + g["pos_x"]
+    gy = g["cell_y"].astype(np.float64) + g["pos_y"]
+    ox = s.cell_x.astype(np.float64) + s.pos_x
+    oy = s.cell_y.astype(np.float64) + s.pos_y
+    checks = {
+        "grid_x": close(gx, ox), "grid_y": close(gy, oy), "pos_z": close(g["pos_z"], s.pos_z),
+        "turb_u": close(g["turb_u"], s.turb_u), "turb_v": close(g["turb_v"], s.turb_v),
+        "turb_w": close(g["turb_w"], s.turb_w), "vel_u": close(g["vel_u"], s.vel_u),
+        "vel_v": close(g["vel_v"], s.vel_v), "vel_w": close(g["vel_w"], s.vel_w),
+        "mass0": close(g["mass"][:, 0], s.mass[0]), "mass1": close(g["mass"][:, 1], s.mass[1]),
+    }
+    for k, ok in checks.items():
+        assert ok.all(), f"{label}: {k} differs at {np.flatnonzero(~ok)[:10]}"
+    assert np.array_equal(g["flags"], s.flags), f"{label}: flags"
+    assert np.array_equal(g["cbt"], s.cbt), f"{label}: cbt"
+
+
+def test_philox_kernel_bit_exact(ctx):
+    u, raw = api.philox_uniforms(ctx, [0, 0], [0, 0, 0, 0], 1)
+    assert list(raw[:4]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    key, ctr = [0xDECAFBAD, 0x12345678], [0xFFFFFFF0, 0xFFFFFFFF, 7, 9]
+    u, raw = api.philox_uniforms(ctx, key, ctr, 5000)
+    ou, oraw = orc.philox_uniforms(key, ctr, 5000)
+    assert np.array_equal(raw, oraw)
+    assert np.array_equal(u, ou)
+
+
+@pytest.mark.parametrize("alpha", [0.0, 0.37, 1.0])
+def test_pbl_diagnostics_matches_oracle(ctx, alpha):
+    spec, frames, _ = small_met()
+    # exercise the fallbacks: missing u*, 1/L, h in some cells
+    s0 = frames[0]["surface"].copy()
+    s1 = frames[1]["surface"].copy()
+    s0["friction_velocity_ms"][::5] = 0.0
+    s1["friction_velocity_ms"][::5] = np.nan
+    s0["inv_obukhov_length_per_m"][::3] = 0.0
+    s1["inv_obukhov_length_per_m"][::3] = 0.0
+    s0["mixing_height_m"][::4] = -1.0
+    s1["mixing_height_m"][::4] = -1.0
+    s0["surface_stress_n_m2"][::7] = 0.0
+    s1["surface_stress_n_m2"][::7] = 0.0
+    surf = api.Surface(ctx, spec.nx, spec.ny)
+    surf.upload(0, s0)
+    surf.upload(1, s1)
+    pbl = api.Pbl(ctx, spec.nx, spec.ny)
+    api.pbl_diagnostics(ctx, surf, alpha, pbl)
+    g = pbl.download()
+    o = orc.pbl_diagnostics(s0, s1, alpha, spec.nx, spec.ny)
+    for k in ("ustar", "wstar", "hmix", "oli", "sshf", "ssr", "surfstr"):
+        ok = close(g[k], getattr(o, k), rel=1e-6)
+        assert ok.all(), (k, np.flatnonzero(~ok)[:5])
+
+
+@pytest.mark.parametrize("n", [1, 255, 4099])
+def test_fused_step_one_step_matches_oracle(ctx, n):
+    spec, frames, met = small_met()
+    alpha = 0.3
+    rec = population(spec.nx, spec.ny, n)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, alpha, rec)
+    prm = production_params(alpha=alpha, counter=(7, 0, 0, 0))
+    nxt = api.step(ctx, p, m, pbl, prm)
+    g = p.download()
+    opbl = pbl_arrays(frames, alpha, spec.nx, spec.ny)
+    s = oracle_step(rec, met, opbl, prm)
+    _compare_state(g, s, f"n={n}")
+    assert nxt == orc.next_counter([7, 0, 0, 0], n, 4)
+    # report the error of both against FP64
+    s64 = oracle_step(rec, met, pbl_arrays(frames, alpha, spec.nx, spec.ny, np.float64), prm, np.float64)
+    act = rec["flags"] == 1
+    if not act.any():
+        return
+    e_gpu = np.max(np.abs(g["pos_z"][act] - s64.pos_z[act]) / np.maximum(np.abs(s64.pos_z[act]), 1.0))
+    e_orc = np.max(np.abs(s.pos_z[act] - s64.pos_z[act]) / np.maximum(np.abs(s64.pos_z[act]), 1.0))
+    print(f"n={n}: max rel |z - z_fp64|: gpu {e_gpu:.2e}, oracle f32 {e_orc:.2e}")
+
+
+@pytest.mark.parametrize("n_sub", [0, 1, 2, 3, 4])
+def test_substep_counts_and_counter_advance(ctx, n_sub):
+    spec, frames, met = small_met(seed=9)
+    rec = population(spec.nx, spec.ny, 700, seed=n_sub)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.5, rec)
+    prm = production_params(alpha=0.5, n_substeps=n_sub, counter=(0xFFFFFFFE, 0xFFFFFFFF, 3, 0))
+    nxt = api.step(ctx, p, m, pbl, prm)
+    s = oracle_step(rec, met, pbl_arrays(frames, 0.5, spec.nx, spec.ny), prm)
+    _compare_state(p.download(), s, f"n_sub={n_sub}")
+    assert nxt == orc.next_counter([0xFFFFFFFE, 0xFFFFFFFF, 3, 0], 700, n_sub)
+
+
+def test_legacy_level_index_mode_and_nonmonotonic_heights(ctx):
+    for heights in ("legacy", "nonmono"):
+        spec, frames, met = small_met(nz=8, heights=heights != "legacy")
+        if heights == "nonmono":
+            h = met["heights"].copy()
+            h[3], h[4] = h[4], h[3]
+            met["heights"] = h
+        rec = population(spec.nx, spec.ny, 513, z_max=7.0 if heights == "legacy" else 3000.0)
+        m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.8, rec)
+        prm = production_params(alpha=0.8, stages=1)     # advection only
+        api.step(ctx, p, m, pbl, prm)
+        s = oracle_step(rec, met, None, prm)
+        _compare_state(p.download(), s, heights)
+
+
+def test_seam_functions_one_at_a_time(ctx):
+    spec, frames, met = small_met(seed=4)
+    rec = population(spec.nx, spec.ny, 1000, seed=21, z_max=60.0)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.25, rec)
+    opbl = pbl_arrays(frames, 0.25, spec.nx, spec.ny)
+    s = orc.State.from_records(rec)
+    # advection (gpu/advection.rs:605)
+    api.advect_dual_wind(ctx, p, m, 0.25, 600.0, 2e-5, 3e-5, 1.0)
+    prm = production_params(alpha=0.25, dt_seconds=600.0, x_grid_per_meter=2e-5, y_grid_per_meter=3e-5,
+                            stages=1)
+    orc.step(s, 1000, met, None, prm)
+    _compare_state(p.download(), s, "advect")
+    # fused Hanna + Langevin (gpu/langevin_fused.rs:133)
+    nxt = api.langevin_fused(ctx, p, pbl, 600.0, 2.5e-4, 4, 0.01, (1, 2), (5, 0, 0, 0))
+    prm = production_params(stages=2, turb_dt_seconds=600.0, rho_grad_over_rho=2.5e-4, key=(1, 2),
+                            counter=(5, 0, 0, 0))
+    orc.step(s, 1000, met, opbl, prm)
+    _compare_state(p.download(), s, "langevin")
+    assert nxt == orc.next_counter([5, 0, 0, 0], 1000, 4)
+    # dry deposition with per-slot velocities and probability output (gpu/deposition.rs:315)
+    vd = np.linspace(-0.001, 0.05, 1000).astype(np.float32)
+    dvd = api.DeviceArray.from_numpy(ctx, vd)
+    dprob = api.DeviceArray(ctx, 1000)
+    api.dry_deposition(ctx, p, dvd, 600.0, 15.0, dprob)
+    oprob = np.zeros(1000, np.float32)
+    prm = production_params(stages=4, turb_dt_seconds=600.0, dry_mode=2)
+    orc.step(s, 1000, met, None, prm, dry_velocity=vd, dry_prob=oprob)
+    _compare_state(p.download(), s, "dry")
+    assert close(dprob.numpy(), oprob).all()
+    # wet deposition (gpu/wet_deposition.rs:368)
+    lam = np.linspace(0, 3e-3, 1000).astype(np.float32)
+    fr = np.linspace(-0.2, 1.3, 1000).astype(np.float32)
+    dl, df, wprob = api.DeviceArray.from_numpy(ctx, lam), api.DeviceArray.from_numpy(ctx, fr), api.DeviceArray(ctx, 1000)
+    api.wet_deposition(ctx, p, dl, df, 600.0, wprob)
+    owprob = np.zeros(1000, np.float32)
+    prm = production_params(stages=8, turb_dt_seconds=600.0, dry_mode=0, wet_mode=2)
+    orc.step(s, 1000, met, None, prm, wet_lambda=lam, wet_fraction=fr, wet_prob=owprob)
+    _compare_state(p.download(), s, "wet")
+    assert close(wprob.numpy(), owprob).all()
+
+
+def test_per_cell_wet_forcing_from_precipitation(ctx):
+    spec, frames, met = small_met(seed=6)
+    rec = population(spec.nx, spec.ny, 3000, seed=8)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.1, rec)
+    rng = np.random.default_rng(2)
+    lsp = np.where(rng.random(spec.nx * spec.ny) < 0.3, rng.lognormal(-1, 1, spec.nx * spec.ny), 0).astype(np.float32)
+    conv = np.where(rng.random(spec.nx * spec.ny) < 0.1, rng.uniform(0, 30, spec.nx * spec.ny), 0).astype(np.float32)
+    cc = rng.uniform(0, 1, spec.nx * spec.ny).astype(np.float32)
+    cf = api.CellField(ctx, spec.nx, spec.ny)
+    cf.from_precipitation(lsp, conv, cc, 1e-4, 0.8)
+    lam, fr = orc.wet_cells(lsp, conv, cc, 1e-4, 0.8)
+    prm = production_params(alpha=0.1, wet_mode=3)
+    api.step(ctx, p, m, pbl, prm, wet_cells=cf)
+    s = oracle_step(rec, met, pbl_arrays(frames, 0.1, spec.nx, spec.ny), prm, wet_cells_lf=(lam, fr),
+                    wet_shape=(spec.nx, spec.ny))
+    _compare_state(p.download(), s, "per-cell wet")
+
+
+def test_empty_and_all_inactive(ctx):
+    spec, frames, met = small_met()
+    rec = population(spec.nx, spec.ny, 300)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.0, rec)
+    p.dispatch_count = 0
+    prm = production_params(counter=(9, 0, 0, 0))
+    assert api.step(ctx, p, m, pbl, prm) == [9, 0, 0, 0]       # empty: Ok, counter unchanged
+    assert np.array_equal(p.download(), rec)
+    rec2 = rec.copy()
+    rec2["flags"] = 0
+    p.dispatch_count = 300
+    p.upload(rec2)
+    api.step(ctx, p, m, pbl, prm)
+    assert np.array_equal(p.download(), rec2)
+
+
+def test_error_codes_mirror_reference(ctx):
+    spec, frames, met = small_met()
+    rec = population(spec.nx, spec.ny, 10)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.0, rec)
+    with pytest.raises(api._lib.FpgError) as e:
+        api.step(ctx, p, m, pbl, production_params(turb_dt_seconds=0.0))
+    assert e.value.status == -2          # InvalidTimeStep (langevin_fused.rs:147)
+    with pytest.raises(api._lib.FpgError) as e:
+        api.step(ctx, p, m, pbl, production_params(dt_seconds=float("nan"), stages=1))
+    assert e.value.status == -2          # gpu/advection.rs:618
+    with pytest.raises(api._lib.FpgError) as e:
+        api.step(ctx, p, m, pbl, production_params(dry_reference_height_m=0.0, stages=4))
+    assert e.value.status == -8          # InvalidReferenceHeight
+    with pytest.raises(api._lib.FpgError) as e:
+        api.Met(ctx, 0, 4, 4)
+    assert e.value.status == -3          # ZeroShape
+    m2 = api.Met(ctx, 4, 4, 4)
+    with pytest.raises(api._lib.FpgError) as e:
+        api.step(ctx, p, m2, pbl, production_params(stages=1))
+    assert e.value.status == -11         # bracket never uploaded
+    g = api.Grid(ctx, 4, 4, 2)
+    with pytest.raises(api._lib.FpgError) as e:
+        g.accumulate(p, species=4)
+    assert e.value.status == -6          # InvalidSpeciesIndex
+    with pytest.raises(api._lib.FpgError) as e:
+        g.accumulate(p, mass_scale=0.0)
+    assert e.value.status == -7          # InvalidMassScale
+    # the failed calls left the particles untouched
+    assert np.array_equal(p.download(), rec)
