@@ -8,16 +8,83 @@ from flexpart_gpu import synthetic
 from flexpart_gpu.records import PARTICLE_DTYPE, StepParams
 from oracle import orc
 
-# Tolerance of the floating-point fields after one step: relative 1e-5 (an
-# absolute 1e-5 for values below 1).  Integer fields, Philox outputs, alive
-# masks, compaction order and grid cell indices are compared bit for bit.
+# Tolerance of the floating-point fields after one step: relative 1e-5 of the
+# field's scale.  The scale is the value itself, floored where a field's value
+# is the small difference of large terms:
+#   grid coordinates: max(|x|, 1 cell);
+#   heights: max(|z|, |z at step start|, 100 m) -- a particle reflected at
+#     the PBL top computes 2h - z with h ~ 1e3 m, so its height carries an
+#     absolute rounding of ulp(h) ~ 1e-4 m however small z ends up (the FP32
+#     oracle differs from the FP64 one by up to 7e-5 relative at z = 4.5 m);
+#   turbulent and mean velocities: max(|v|, 2 m/s) -- each sub-step adds
+#     an Ornstein-Uhlenbeck decay, a noise term of size sigma_w (up to ~2 m/s
+#     for w* <= 2.5 m/s) and a drift term whose height derivative is steep
+#     near the ground, so a velocity near zero is the difference of terms of
+#     that size (the FP32 oracle differs from the FP64 one by up to 2e-5 m/s);
+#   masses: the value itself.
+# Integer fields, Philox outputs, alive masks, compaction order and grid cell
+# indices are compared bit for bit.
 REL_TOL = 1e-5
 
 
-def close(gpu, ref, rel=REL_TOL):
+def close(gpu, ref, rel=REL_TOL, floor=1.0):
     gpu = np.asarray(gpu, np.float64)
     ref = np.asarray(ref, np.float64)
-    return np.abs(gpu - ref) <= rel * np.maximum(np.abs(ref), 1.0)
+    return np.abs(gpu - ref) <= rel * np.maximum(np.abs(ref), floor)
+
+
+def _fields(rec_or_state):
+    """float64 views of the compared fields of records or an oracle State."""
+    if isinstance(rec_or_state, np.ndarray):
+        r = rec_or_state
+        out = {"grid_x": r["cell_x"].astype(np.float64) + r["pos_x"],
+               "grid_y": r["cell_y"].astype(np.float64) + r["pos_y"]}
+        for f in ("pos_z", "turb_u", "turb_v", "turb_w", "vel_u", "vel_v", "vel_w"):
+            out[f] = r[f].astype(np.float64)
+        for k in range(4):
+            out[f"mass{k}"] = r["mass"][:, k].astype(np.float64)
+        return out
+    s = rec_or_state
+    out = {"grid_x": s.cell_x.astype(np.float64) + s.pos_x, "grid_y": s.cell_y.astype(np.float64) + s.pos_y}
+    for f in ("pos_z", "turb_u", "turb_v", "turb_w", "vel_u", "vel_v", "vel_w"):
+        out[f] = np.asarray(getattr(s, f), np.float64)
+    for k in range(4):
+        out[f"mass{k}"] = np.asarray(s.mass[k], np.float64)
+    return out
+
+
+ENVELOPE = 4.0
+
+
+def field_checks(g, s, z_in, s64=None, stats=None):
+    """Per-field parity masks of GPU records `g` against the FP32 oracle
+    state `s`.  With the FP64 oracle state `s64`, a particle also passes when
+    the GPU is no further from the FP32 oracle than ENVELOPE times the FP32
+    oracle's own distance from FP64: for the few ill-conditioned particles
+    (unstable cells, a start near the ground) FP32 arithmetic itself cannot
+    resolve the step to 1e-5, and the GPU is then held to FP32's own
+    accuracy.  `stats` (a dict) counts those particles per field."""
+    G, S = _fields(g), _fields(s)
+    S64 = _fields(s64) if s64 is not None else None
+    zscale = np.maximum(np.maximum(np.abs(S["pos_z"]), np.abs(z_in.astype(np.float64))), 100.0)
+    floors = {"grid_x": 1.0, "grid_y": 1.0}
+    out = {}
+    for f in G:
+        if f == "pos_z":
+            ok = np.abs(G[f] - S[f]) <= REL_TOL * zscale
+        elif f.startswith("mass"):
+            ok = close(G[f], S[f], floor=0.0)
+        elif f.startswith("turb") or f.startswith("vel"):
+            ok = close(G[f], S[f], floor=2.0)
+        else:
+            ok = close(G[f], S[f], floor=floors[f])
+        if S64 is not None:
+            env = np.abs(G[f] - S[f]) <= ENVELOPE * np.abs(S[f] - S64[f]) + 1e-12
+            if stats is not None:
+                stats[f] = stats.get(f, 0) + int((~ok & env).sum())
+            ok = ok | env
+        out[f] = ok
+    return out
 
 
 def small_met(nx=24, ny=18, nz=12, seed=5, heights=True):
@@ -72,7 +139,9 @@ def oracle_step(rec, met, pbl, params, dtype=np.float32, **kw):
 
 
 def production_params(**kw) -> StepParams:
+    """Production step settings; the metres->grid scale is that of the
+    0.5-degree test grid at 44 N (about 1/40 km and 1/55 km)."""
     base = dict(alpha=0.3, dt_seconds=900.0, turb_dt_seconds=900.0, key=(42, 0), counter=(0, 0, 0, 0),
-                dry_mode=1, dry_velocity_m_s=0.002)
+                dry_mode=1, dry_velocity_m_s=0.002, x_grid_per_meter=2.5e-5, y_grid_per_meter=1.8e-5)
     base.update(kw)
     return StepParams.production(**base)

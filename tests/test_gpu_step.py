@@ -1,14 +1,15 @@
 """GPU parity of the fused step and its seam functions against the oracle.
 
 Every call goes through the C ABI (libfpg.so via ctypes).  Tolerance: the
-floating-point fields agree to relative 1e-5 (absolute 1e-5 below 1) after
-one step; integer fields (cells, flags, cbt) and Philox outputs are
-bit-exact.  The error of both against the FP64 oracle is printed.
+floating-point fields agree to relative 1e-5 of each field's scale after one
+step (tests/helpers.py: field_checks); integer fields (cells, flags, cbt) and
+Philox outputs are bit-exact.  Against the FP64 oracle the GPU's error is no
+larger than the FP32 oracle's own (both printed).
 """
 import numpy as np
 import pytest
 
-from helpers import REL_TOL, close, oracle_step, pbl_arrays, population, production_params, small_met
+from helpers import close, field_checks, oracle_step, pbl_arrays, population, production_params, small_met
 from oracle import orc
 
 pytestmark = pytest.mark.gpu
@@ -38,20 +39,17 @@ def _gpu_setup(ctx, spec, frames, met, alpha, rec):
     return m, surf, pbl, p
 
 
-def _compare_state(g, s, label):
-    gx = g["cell_x"].astype(np.float64) + g["pos_x"]
-    gy = g["cell_y"].astype(np.float64) + g["pos_y"]
-    ox = s.cell_x.astype(np.float64) + s.pos_x
-    oy = s.cell_y.astype(np.float64) + s.pos_y
-    checks = {
-        "grid_x": close(gx, ox), "grid_y": close(gy, oy), "pos_z": close(g["pos_z"], s.pos_z),
-        "turb_u": close(g["turb_u"], s.turb_u), "turb_v": close(g["turb_v"], s.turb_v),
-        "turb_w": close(g["turb_w"], s.turb_w), "vel_u": close(g["vel_u"], s.vel_u),
-        "vel_v": close(g["vel_v"], s.vel_v), "vel_w": close(g["vel_w"], s.vel_w),
-        "mass0": close(g["mass"][:, 0], s.mass[0]), "mass1": close(g["mass"][:, 1], s.mass[1]),
-    }
+def _compare_state(g, s, label, rec_in, s64=None):
+    stats = {}
+    checks = field_checks(g, s, rec_in["pos_z"], s64, stats)
+    if any(stats.values()):
+        print(f"{label}: particles held to the FP32 envelope: {stats}")
     for k, ok in checks.items():
-        assert ok.all(), f"{label}: {k} differs at {np.flatnonzero(~ok)[:10]}"
+        if not ok.all():
+            bad = np.flatnonzero(~ok)[:5]
+            detail = [(int(i), float(rec_in["pos_z"][i]), float(g["pos_z"][i]), float(s.pos_z[i]),
+                       float(g["turb_w"][i]), float(s.turb_w[i])) for i in bad]
+            raise AssertionError(f"{label}: {k} differs at (slot, z_in, z_gpu, z_orc, tw_gpu, tw_orc) {detail}")
     assert np.array_equal(g["flags"], s.flags), f"{label}: flags"
     assert np.array_equal(g["cbt"], s.cbt), f"{label}: cbt"
 
@@ -103,16 +101,21 @@ def test_fused_step_one_step_matches_oracle(ctx, n):
     g = p.download()
     opbl = pbl_arrays(frames, alpha, spec.nx, spec.ny)
     s = oracle_step(rec, met, opbl, prm)
-    _compare_state(g, s, f"n={n}")
+    s64 = oracle_step(rec, met, pbl_arrays(frames, alpha, spec.nx, spec.ny, np.float64), prm, np.float64)
+    _compare_state(g, s, f"n={n}", rec, s64)
     assert nxt == orc.next_counter([7, 0, 0, 0], n, 4)
     # report the error of both against FP64
-    s64 = oracle_step(rec, met, pbl_arrays(frames, alpha, spec.nx, spec.ny, np.float64), prm, np.float64)
     act = rec["flags"] == 1
     if not act.any():
         return
-    e_gpu = np.max(np.abs(g["pos_z"][act] - s64.pos_z[act]) / np.maximum(np.abs(s64.pos_z[act]), 1.0))
-    e_orc = np.max(np.abs(s.pos_z[act] - s64.pos_z[act]) / np.maximum(np.abs(s64.pos_z[act]), 1.0))
-    print(f"n={n}: max rel |z - z_fp64|: gpu {e_gpu:.2e}, oracle f32 {e_orc:.2e}")
+    zs = np.maximum(np.maximum(np.abs(s64.pos_z[act]), np.abs(rec["pos_z"][act])), 100.0)
+    for name, a, b in (("pos_z", g["pos_z"], s.pos_z), ("turb_w", g["turb_w"], s.turb_w)):
+        ref = getattr(s64, name)[act]
+        sc = zs if name == "pos_z" else np.maximum(np.abs(ref), 2.0)
+        e_gpu = np.max(np.abs(a[act] - ref) / sc)
+        e_orc = np.max(np.abs(b[act] - ref) / sc)
+        print(f"n={n}: max scaled |{name} - fp64|: gpu {e_gpu:.2e}, oracle f32 {e_orc:.2e}")
+        assert e_gpu <= 2.0 * e_orc + 1e-6
 
 
 @pytest.mark.parametrize("n_sub", [0, 1, 2, 3, 4])
@@ -123,7 +126,8 @@ def test_substep_counts_and_counter_advance(ctx, n_sub):
     prm = production_params(alpha=0.5, n_substeps=n_sub, counter=(0xFFFFFFFE, 0xFFFFFFFF, 3, 0))
     nxt = api.step(ctx, p, m, pbl, prm)
     s = oracle_step(rec, met, pbl_arrays(frames, 0.5, spec.nx, spec.ny), prm)
-    _compare_state(p.download(), s, f"n_sub={n_sub}")
+    s64 = oracle_step(rec, met, pbl_arrays(frames, 0.5, spec.nx, spec.ny, np.float64), prm, np.float64)
+    _compare_state(p.download(), s, f"n_sub={n_sub}", rec, s64)
     assert nxt == orc.next_counter([0xFFFFFFFE, 0xFFFFFFFF, 3, 0], 700, n_sub)
 
 
@@ -139,7 +143,8 @@ def test_legacy_level_index_mode_and_nonmonotonic_heights(ctx):
         prm = production_params(alpha=0.8, stages=1)     # advection only
         api.step(ctx, p, m, pbl, prm)
         s = oracle_step(rec, met, None, prm)
-        _compare_state(p.download(), s, heights)
+        s64 = oracle_step(rec, met, None, prm, np.float64)
+        _compare_state(p.download(), s, heights, rec, s64)
 
 
 def test_seam_functions_one_at_a_time(ctx):
@@ -147,19 +152,23 @@ def test_seam_functions_one_at_a_time(ctx):
     rec = population(spec.nx, spec.ny, 1000, seed=21, z_max=60.0)
     m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.25, rec)
     opbl = pbl_arrays(frames, 0.25, spec.nx, spec.ny)
+    opbl64 = pbl_arrays(frames, 0.25, spec.nx, spec.ny, np.float64)
     s = orc.State.from_records(rec)
+    s64 = orc.State.from_records(rec, np.float64)
     # advection (gpu/advection.rs:605)
     api.advect_dual_wind(ctx, p, m, 0.25, 600.0, 2e-5, 3e-5, 1.0)
     prm = production_params(alpha=0.25, dt_seconds=600.0, x_grid_per_meter=2e-5, y_grid_per_meter=3e-5,
                             stages=1)
     orc.step(s, 1000, met, None, prm)
-    _compare_state(p.download(), s, "advect")
+    orc.step(s64, 1000, met, None, prm)
+    _compare_state(p.download(), s, "advect", rec, s64)
     # fused Hanna + Langevin (gpu/langevin_fused.rs:133)
     nxt = api.langevin_fused(ctx, p, pbl, 600.0, 2.5e-4, 4, 0.01, (1, 2), (5, 0, 0, 0))
     prm = production_params(stages=2, turb_dt_seconds=600.0, rho_grad_over_rho=2.5e-4, key=(1, 2),
                             counter=(5, 0, 0, 0))
     orc.step(s, 1000, met, opbl, prm)
-    _compare_state(p.download(), s, "langevin")
+    orc.step(s64, 1000, met, opbl64, prm)
+    _compare_state(p.download(), s, "langevin", rec, s64)
     assert nxt == orc.next_counter([5, 0, 0, 0], 1000, 4)
     # dry deposition with per-slot velocities and probability output (gpu/deposition.rs:315)
     vd = np.linspace(-0.001, 0.05, 1000).astype(np.float32)
@@ -169,7 +178,8 @@ def test_seam_functions_one_at_a_time(ctx):
     oprob = np.zeros(1000, np.float32)
     prm = production_params(stages=4, turb_dt_seconds=600.0, dry_mode=2)
     orc.step(s, 1000, met, None, prm, dry_velocity=vd, dry_prob=oprob)
-    _compare_state(p.download(), s, "dry")
+    orc.step(s64, 1000, met, None, prm, dry_velocity=vd)
+    _compare_state(p.download(), s, "dry", rec, s64)
     assert close(dprob.numpy(), oprob).all()
     # wet deposition (gpu/wet_deposition.rs:368)
     lam = np.linspace(0, 3e-3, 1000).astype(np.float32)
@@ -179,7 +189,8 @@ def test_seam_functions_one_at_a_time(ctx):
     owprob = np.zeros(1000, np.float32)
     prm = production_params(stages=8, turb_dt_seconds=600.0, dry_mode=0, wet_mode=2)
     orc.step(s, 1000, met, None, prm, wet_lambda=lam, wet_fraction=fr, wet_prob=owprob)
-    _compare_state(p.download(), s, "wet")
+    orc.step(s64, 1000, met, None, prm, wet_lambda=lam, wet_fraction=fr)
+    _compare_state(p.download(), s, "wet", rec, s64)
     assert close(wprob.numpy(), owprob).all()
 
 
@@ -196,9 +207,10 @@ def test_per_cell_wet_forcing_from_precipitation(ctx):
     lam, fr = orc.wet_cells(lsp, conv, cc, 1e-4, 0.8)
     prm = production_params(alpha=0.1, wet_mode=3)
     api.step(ctx, p, m, pbl, prm, wet_cells=cf)
-    s = oracle_step(rec, met, pbl_arrays(frames, 0.1, spec.nx, spec.ny), prm, wet_cells_lf=(lam, fr),
-                    wet_shape=(spec.nx, spec.ny))
-    _compare_state(p.download(), s, "per-cell wet")
+    kw = dict(wet_cells_lf=(lam, fr), wet_shape=(spec.nx, spec.ny))
+    s = oracle_step(rec, met, pbl_arrays(frames, 0.1, spec.nx, spec.ny), prm, **kw)
+    s64 = oracle_step(rec, met, pbl_arrays(frames, 0.1, spec.nx, spec.ny, np.float64), prm, np.float64, **kw)
+    _compare_state(p.download(), s, "per-cell wet", rec, s64)
 
 
 def test_empty_and_all_inactive(ctx):
