@@ -393,6 +393,28 @@ fpg_status fpg_compaction_destroy(fpg_compaction* c);
 fpg_status fpg_compact(fpg_ctx* ctx, fpg_particles* particles, fpg_compaction* c,
                        uint32_t* active_count, uint32_t* compacted_indices_dev, void* stream);
 
+/* Largest slot count fpg_compaction_indices_static accepts (65536 tiles of
+ * 2048 slots; its scratch is a 256 KiB static device array). */
+#define FPG_STATIC_COMPACT_MAX_SLOTS (65536u * 2048u)
+
+/* No counterpart in the reference.  The stable compaction scan of
+ * fpg_compact for callers that cannot allocate device memory (their device
+ * memory belongs to another allocator, or an allocation would stall a
+ * latency-critical loop): it allocates nothing and keeps its per-tile
+ * scratch in a static device array inside the library.  Inputs and outputs
+ * are the caller's device buffers: `flags_dev` (n u32, bit 0 = active),
+ * `indices_dev` (n u32; the first *active_count_dev entries receive the
+ * original slot of each active particle, in slot order) and
+ * `active_count_dev` (one u32).  Particle data is not moved.
+ * n above FPG_STATIC_COMPACT_MAX_SLOTS returns FPG_ERR_VALUE_TOO_LARGE.
+ * The first call for a device looks up the scratch array's device address
+ * (once per device) and should come before any stream capture.  All calls
+ * on a device share the one array: calls that overlap on the GPU race;
+ * calls ordered on one stream are safe. */
+fpg_status fpg_compaction_indices_static(fpg_ctx* ctx, const uint32_t* flags_dev, size_t n,
+                                         uint32_t* indices_dev, uint32_t* active_count_dev,
+                                         void* stream);
+
 /* ------------------------------------------------------------------------
  * Philox utility (philox_rng.wgsl:441-464, src/gpu/rng.rs:198)
  * ---------------------------------------------------------------------- */
