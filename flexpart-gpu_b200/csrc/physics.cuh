@@ -6,8 +6,8 @@
 // as written, and the only fused operation is the explicit fmaf of lerp()
 // (the reference CPU lerp is `a.mul_add(1 - t, b * t)`,
 // src/physics/interpolation.rs:75-77, src/io/temporal.rs:417-420).
-// Transcendentals are CUDA's IEEE-accurate expf/logf/powf/sinf/cosf; sqrtf
-// and '/' are correctly rounded (no fast-math flags).
+// Transcendentals are CUDA's accurate expf/logf/powf/sinf/cosf/cbrtf (no
+// fast-math intrinsics); sqrtf and '/' are correctly rounded.
 #pragma once
 
 #include <cstdint>
@@ -21,6 +21,13 @@ __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fm
 __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(a, 1.0f - t, b * t); }
 __device__ __forceinline__ float sanitize_positive(float v) { return (finitef(v) && v > 0.0f) ? v : 0.0f; }
+
+// x^(1/3), x^(2/3) and x^(-1/3) for x >= 0 from one cbrtf (max 1 ulp): the
+// reference writes pow(x, 1.0/3.0), pow(x, 2.0/3.0), pow(x, -1.0/3.0)
+// (hanna.rs:81-92, langevin_fused.wgsl:247-254,315-321).  The results stay
+// within a few ulp of powf with the f32-rounded exponents (1/3 rounds to
+// 0.33333334, a relative exponent error of 3e-8), at a fraction of its cost.
+__device__ __forceinline__ float pow_third(float x) { return cbrtf(x); }
 
 // ---- Philox4x32-10 (src/physics/rng.rs:28-65, langevin_fused.wgsl:126-169) --
 struct u32x4 { uint32_t x, y, z, w; };
@@ -92,13 +99,14 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
         tlv = tlu;
         tlw = tlu;
     } else if (ol < 0.0f) {
-        sigu = 1.0e-2f + ust * powf(12.0f - 0.5f * h / ol, 1.0f / 3.0f);
+        sigu = 1.0e-2f + ust * pow_third(12.0f - 0.5f * h / ol);
         sigv = sigu;
-        const float z23 = powf(zeta, 2.0f / 3.0f);
+        const float c = pow_third(zeta);
+        const float z23 = c * c;
         const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
         sigw = sqrtf(sigw_sq) + 1.0e-2f;
-        dsigwdz = 0.5f / sigw / h *
-                  (-1.4f * ust * ust + wst * wst * (0.8f * powf(fmaxf(zeta, 1.0e-3f), -(1.0f / 3.0f)) - 1.8f * z23));
+        const float zm13 = 1.0f / (zeta >= 1.0e-3f ? c : pow_third(1.0e-3f));
+        dsigwdz = 0.5f / sigw / h * (-1.4f * ust * ust + wst * wst * (0.8f * zm13 - 1.8f * z23));
         tlu = 0.15f * h / sigu;
         tlv = tlu;
         if (z < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * fabsf(z / ol)));
@@ -147,11 +155,12 @@ __device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float 
         sigw = sigw + 1.0e-2f;
         tlw = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
     } else if (ol < 0.0f) {
-        const float z23 = powf(zeta, 2.0f / 3.0f);
+        const float c = pow_third(zeta);
+        const float z23 = c * c;
         const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
         sigw = sqrtf(sigw_sq) + 1.0e-2f;
-        dsigwdz = 0.5f / sigw / h *
-                  (-1.4f * ust * ust + wst * wst * (0.8f * powf(fmaxf(zeta, 1.0e-3f), -(1.0f / 3.0f)) - 1.8f * z23));
+        const float zm13 = 1.0f / (zeta >= 1.0e-3f ? c : pow_third(1.0e-3f));
+        dsigwdz = 0.5f / sigw / h * (-1.4f * ust * ust + wst * wst * (0.8f * zm13 - 1.8f * z23));
         if (z < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * fabsf(z / ol)));
         else if (zeta < 0.1f) tlw = 0.59f * z / sigw;
         else tlw = 0.15f * h / sigw * (1.0f - expf(-5.0f * zeta));

@@ -106,14 +106,25 @@ __device__ __forceinline__ void axis_bracket(float coord, uint32_t n, uint32_t& 
     t = c - lf;
 }
 
-__device__ __forceinline__ float tri(float c000, float c100, float c010, float c110, float c001, float c101,
-                                     float c011, float c111, float tx, float ty, float tz) {
-    return lerpf(lerpf(lerpf(c000, c100, tx), lerpf(c010, c110, tx), ty),
-                 lerpf(lerpf(c001, c101, tx), lerpf(c011, c111, tx), ty), tz);
+// sample_dual_{u,v,w} (advection_dual_wind.wgsl:142-236): trilinear in each
+// frame, then lerp by alpha.  The x-lerps of one (y, z) corner pair are taken
+// as soon as its four float4 (2 nodes x 2 frames) arrive, which keeps the
+// live registers at 16 floats instead of 64 while giving the same roundings
+// in the same order as the reference expression.
+struct Lerp6 { float u0, v0, w0, u1, v1, w1; };
+
+__device__ __forceinline__ Lerp6 xpair(const float4* br, uint32_t na, uint32_t nb, float tx) {
+    const float4 a0 = __ldg(br + 2u * na), a1 = __ldg(br + 2u * na + 1u);
+    const float4 b0 = __ldg(br + 2u * nb), b1 = __ldg(br + 2u * nb + 1u);
+    return Lerp6{lerpf(a0.x, b0.x, tx), lerpf(a0.y, b0.y, tx), lerpf(a0.z, b0.z, tx),
+                 lerpf(a1.x, b1.x, tx), lerpf(a1.y, b1.y, tx), lerpf(a1.z, b1.z, tx)};
 }
 
-// sample_dual_{u,v,w} (advection_dual_wind.wgsl:142-236): trilinear in each
-// frame, then lerp by alpha.
+__device__ __forceinline__ Lerp6 lerp6(const Lerp6& a, const Lerp6& b, float t) {
+    return Lerp6{lerpf(a.u0, b.u0, t), lerpf(a.v0, b.v0, t), lerpf(a.w0, b.w0, t),
+                 lerpf(a.u1, b.u1, t), lerpf(a.v1, b.v1, t), lerpf(a.w1, b.w1, t)};
+}
+
 __device__ __forceinline__ float3 sample_dual(const StepArgs& a, const float* hts, float x, float y, float z) {
     uint32_t x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
@@ -123,22 +134,15 @@ __device__ __forceinline__ float3 sample_dual(const StepArgs& a, const float* ht
     const uint32_t c00 = (x0 * a.ny + y0) * a.nz, c10 = (x1 * a.ny + y0) * a.nz;
     const uint32_t c01 = (x0 * a.ny + y1) * a.nz, c11 = (x1 * a.ny + y1) * a.nz;
     const float4* br = a.bracket;
-    const float4 p000 = __ldg(br + 2u * (c00 + z0)), q000 = __ldg(br + 2u * (c00 + z0) + 1u);
-    const float4 p100 = __ldg(br + 2u * (c10 + z0)), q100 = __ldg(br + 2u * (c10 + z0) + 1u);
-    const float4 p010 = __ldg(br + 2u * (c01 + z0)), q010 = __ldg(br + 2u * (c01 + z0) + 1u);
-    const float4 p110 = __ldg(br + 2u * (c11 + z0)), q110 = __ldg(br + 2u * (c11 + z0) + 1u);
-    const float4 p001 = __ldg(br + 2u * (c00 + z1)), q001 = __ldg(br + 2u * (c00 + z1) + 1u);
-    const float4 p101 = __ldg(br + 2u * (c10 + z1)), q101 = __ldg(br + 2u * (c10 + z1) + 1u);
-    const float4 p011 = __ldg(br + 2u * (c01 + z1)), q011 = __ldg(br + 2u * (c01 + z1) + 1u);
-    const float4 p111 = __ldg(br + 2u * (c11 + z1)), q111 = __ldg(br + 2u * (c11 + z1) + 1u);
-    float3 r;
-    r.x = lerpf(tri(p000.x, p100.x, p010.x, p110.x, p001.x, p101.x, p011.x, p111.x, tx, ty, tz),
-                tri(q000.x, q100.x, q010.x, q110.x, q001.x, q101.x, q011.x, q111.x, tx, ty, tz), a.alpha);
-    r.y = lerpf(tri(p000.y, p100.y, p010.y, p110.y, p001.y, p101.y, p011.y, p111.y, tx, ty, tz),
-                tri(q000.y, q100.y, q010.y, q110.y, q001.y, q101.y, q011.y, q111.y, tx, ty, tz), a.alpha);
-    r.z = lerpf(tri(p000.z, p100.z, p010.z, p110.z, p001.z, p101.z, p011.z, p111.z, tx, ty, tz),
-                tri(q000.z, q100.z, q010.z, q110.z, q001.z, q101.z, q011.z, q111.z, tx, ty, tz), a.alpha);
-    return r;
+    // lerp(lerp(lerp(c000,c100,tx), lerp(c010,c110,tx), ty), lerp(lerp(c001,c101,tx), lerp(c011,c111,tx), ty), tz)
+    const Lerp6 l00 = xpair(br, c00 + z0, c10 + z0, tx);
+    const Lerp6 l10 = xpair(br, c01 + z0, c11 + z0, tx);
+    const Lerp6 l0 = lerp6(l00, l10, ty);
+    const Lerp6 l01 = xpair(br, c00 + z1, c10 + z1, tx);
+    const Lerp6 l11 = xpair(br, c01 + z1, c11 + z1, tx);
+    const Lerp6 l1 = lerp6(l01, l11, ty);
+    const Lerp6 t = lerp6(l0, l1, tz);
+    return make_float3(lerpf(t.u0, t.u1, a.alpha), lerpf(t.v0, t.v1, a.alpha), lerpf(t.w0, t.w1, a.alpha));
 }
 
 // split_horizontal_coord (advection_dual_wind.wgsl:238-248).
@@ -151,7 +155,7 @@ __device__ __forceinline__ void split_coord(float coord, uint32_t n, int32_t& ce
     frac = f;
 }
 
-__global__ void __launch_bounds__(256) fused_step_kernel(StepArgs a) {
+__global__ void __launch_bounds__(256, 4) fused_step_kernel(StepArgs a) {
     extern __shared__ float s_heights[];
     if (a.stages & FPG_STAGE_ADVECT) {
         for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];

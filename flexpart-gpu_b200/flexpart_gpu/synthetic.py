@@ -211,7 +211,9 @@ def particles_at_sources(scn: Scenario, n: int, seed: int = 3) -> np.ndarray:
     rng = np.random.default_rng(seed)
     spec = scn.met
     rec = np.zeros(n, PARTICLE_DTYPE)
-    src_idx = rng.integers(0, len(scn.sources), n)
+    # consecutive slots belong to one source, as the release manager fills
+    # them (release/mod.rs:103-146)
+    src_idx = np.sort(rng.integers(0, len(scn.sources), n))
     lon = np.array([s.lon for s in scn.sources])[src_idx] + rng.normal(0, 3.0 * spec.dx_deg, n)
     lat = np.array([s.lat for s in scn.sources])[src_idx] + rng.normal(0, 3.0 * spec.dy_deg, n)
     x = np.clip((lon - spec.xlon0) / spec.dx_deg, 0, spec.nx - 1.001)
