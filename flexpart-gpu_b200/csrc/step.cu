@@ -113,11 +113,23 @@ __device__ __forceinline__ void axis_bracket(float coord, uint32_t n, uint32_t& 
 // in the same order as the reference expression.
 struct Lerp6 { float u0, v0, w0, u1, v1, w1; };
 
+// One bracket node (t0 u,v,w,0 | t1 u,v,w,0) is 32 bytes at a 32-byte
+// aligned offset (cudaMalloc base, node stride 32 B): one 256-bit load.
+struct Node { float u0, v0, w0, p0, u1, v1, w1, p1; };
+
+__device__ __forceinline__ Node ld_node(const float4* br, uint32_t n) {
+    Node v;
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(v.u0), "=f"(v.v0), "=f"(v.w0), "=f"(v.p0), "=f"(v.u1), "=f"(v.v1), "=f"(v.w1), "=f"(v.p1)
+        : "l"(br + 2u * n));
+    return v;
+}
+
 __device__ __forceinline__ Lerp6 xpair(const float4* br, uint32_t na, uint32_t nb, float tx) {
-    const float4 a0 = __ldg(br + 2u * na), a1 = __ldg(br + 2u * na + 1u);
-    const float4 b0 = __ldg(br + 2u * nb), b1 = __ldg(br + 2u * nb + 1u);
-    return Lerp6{lerpf(a0.x, b0.x, tx), lerpf(a0.y, b0.y, tx), lerpf(a0.z, b0.z, tx),
-                 lerpf(a1.x, b1.x, tx), lerpf(a1.y, b1.y, tx), lerpf(a1.z, b1.z, tx)};
+    const Node a = ld_node(br, na);
+    const Node b = ld_node(br, nb);
+    return Lerp6{lerpf(a.u0, b.u0, tx), lerpf(a.v0, b.v0, tx), lerpf(a.w0, b.w0, tx),
+                 lerpf(a.u1, b.u1, tx), lerpf(a.v1, b.v1, tx), lerpf(a.w1, b.w1, tx)};
 }
 
 __device__ __forceinline__ Lerp6 lerp6(const Lerp6& a, const Lerp6& b, float t) {

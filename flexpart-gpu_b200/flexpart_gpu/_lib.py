@@ -106,6 +106,9 @@ _sig("fpg_compaction_destroy", _i32, _vp)
 _sig("fpg_compact", _i32, _vp, _vp, _vp, _u32p, _vp, _vp)
 _sig("fpg_philox_uniforms", _i32, _vp, _u32p, _u32p, _sz, _vp, _vp, _vp)
 _sig("fpg_compaction_indices_static", _i32, _vp, _vp, _sz, _vp, _vp, _vp)
+_sig("fpg_sorter_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_sorter_destroy", _i32, _vp)
+_sig("fpg_sort_by_cell", _i32, _vp, _vp, _vp, _vp, _vp, _vp)
 
 
 def check(status: int, what: str) -> None:
@@ -133,4 +136,5 @@ EXPORTED = [
     "fpg_compaction_create", "fpg_compaction_destroy", "fpg_compact",
     "fpg_philox_uniforms",
     "fpg_compaction_indices_static",
+    "fpg_sorter_create", "fpg_sorter_destroy", "fpg_sort_by_cell",
 ]

@@ -368,6 +368,27 @@ class Compaction:
         return int(cnt.value)
 
 
+class Sorter:
+    """fpg_sorter: stable reorder of particles by 3-D met cell."""
+
+    def __init__(self, ctx: Context, capacity: int):
+        self.ctx = ctx
+        h = _vp()
+        check(lib.fpg_sorter_create(ctx.h, capacity, ctypes.byref(h)), "fpg_sorter_create")
+        self.h = h
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib.fpg_sorter_destroy(self.h)
+        except Exception:
+            pass
+
+    def sort(self, particles: Particles, met: Met, perm: DeviceArray | None = None, stream=None):
+        check(lib.fpg_sort_by_cell(self.ctx.h, particles.h, met.h, self.h, _vp(perm.ptr) if perm else None, stream),
+              "fpg_sort_by_cell")
+
+
 def philox_uniforms(ctx: Context, key, counter, n_blocks: int):
     out = DeviceArray(ctx, 4 * n_blocks, np.float32)
     raw = DeviceArray(ctx, 4 * n_blocks, np.uint32)

@@ -393,6 +393,28 @@ fpg_status fpg_compaction_destroy(fpg_compaction* c);
 fpg_status fpg_compact(fpg_ctx* ctx, fpg_particles* particles, fpg_compaction* c,
                        uint32_t* active_count, uint32_t* compacted_indices_dev, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Spatial reorder by met cell (replaces the reference's optional host Morton
+ * sort: ParticleStore::sort_spatially, src/particles/mod.rs:649-699, applied
+ * by apply_spatial_sort_if_enabled, src/simulation/timeloop.rs:1414-1430)
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_sorter fpg_sorter;
+
+fpg_status fpg_sorter_create(fpg_ctx* ctx, size_t capacity, fpg_sorter** out);
+fpg_status fpg_sorter_destroy(fpg_sorter* s);
+/* Stable reorder of slots [0, dispatch_count) by the 3-D met cell of each
+ * particle, key ((ix*ny)+iy)*nz+iz with ix = floor(clamp(cell_x+pos_x, 0,
+ * nx-1)), iy likewise, iz = floor(clamp(level(pos_z), 0, nz-1)) and level()
+ * the metres->level map of the advection (advection_dual_wind.wgsl:94-117);
+ * inactive slots sort last, as the reference's INACTIVE_MORTON_KEY
+ * (particles/mod.rs:27).  All fields move; slots >= dispatch_count keep
+ * their place.  `perm_dev` (optional, dispatch_count u32) receives the old
+ * slot of each new slot.  Philox streams follow the new slot, as they do
+ * after the reference's own sort.  Field pointers change (the handle swaps
+ * to the sorter's second block). */
+fpg_status fpg_sort_by_cell(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met, fpg_sorter* sorter,
+                            uint32_t* perm_dev, void* stream);
+
 /* Largest slot count fpg_compaction_indices_static accepts (65536 tiles of
  * 2048 slots; its scratch is a 256 KiB static device array). */
 #define FPG_STATIC_COMPACT_MAX_SLOTS (65536u * 2048u)

@@ -430,6 +430,27 @@ def compact_records(rec: np.ndarray):
     return out, count, idx
 
 
+def cell_keys(state: State, n, heights, shape):
+    """Met-cell keys of the spatial reorder (inactive: nx*ny*nz)."""
+    nx, ny, nz = shape
+    h = np.ascontiguousarray(heights, np.float32)
+    keys = np.zeros(max(n, 1), np.uint32)
+    getattr(lib, "orc_cell_keys" + _sfx(state.dtype))(
+        ctypes.c_size_t(n), _ptr(state.cell_x), _ptr(state.cell_y), _ptr(state.pos_x), _ptr(state.pos_y),
+        _ptr(state.pos_z), _ptr(state.flags), _ptr(h), ctypes.c_size_t(nx), ctypes.c_size_t(ny),
+        ctypes.c_size_t(nz), _ptr(keys))
+    return keys[:n]
+
+
+def sort_by_cell(rec: np.ndarray, n, heights, shape):
+    """Stable reorder of records [0, n) by met-cell key; returns (records, perm)."""
+    keys = cell_keys(State.from_records(rec[:n]), n, heights, shape)
+    perm = np.argsort(keys, kind="stable").astype(np.uint32)
+    out = rec.copy()
+    out[:n] = rec[:n][perm]
+    return out, perm
+
+
 def interpolation_alpha(t0, t1, target, clamp=True):
     out = ctypes.c_float()
     st = lib.orc_interpolation_alpha(ctypes.c_int64(t0), ctypes.c_int64(t1), ctypes.c_int64(target),

@@ -84,3 +84,29 @@ def test_compaction_matches_reference_sets_and_order(ctx, n, inactive):
     assert p.dispatch_count == count_ref
     assert np.array_equal(idx.numpy()[:count], idx_ref)
     assert np.array_equal(p.download(), out_ref)
+
+
+@pytest.mark.parametrize("n,heights", [(100_003, True), (4_097, False)])
+def test_sort_by_cell_matches_oracle_permutation(ctx, n, heights):
+    from helpers import production_params, small_met
+    spec, frames, met = small_met(nz=16, heights=heights)
+    rec = population(spec.nx, spec.ny, n, seed=5, z_max=3000.0 if heights else 15.0)
+    rec["time"] = np.arange(n, dtype=np.int32)
+    p = api.Particles(ctx, n)
+    p.upload(rec)
+    m = api.Met(ctx, spec.nx, spec.ny, spec.nz)
+    m.upload_frame(0, met["u0"], met["v0"], met["w0"])
+    m.upload_frame(1, met["u1"], met["v1"], met["w1"])
+    m.set_level_heights(met["heights"])
+    srt = api.Sorter(ctx, n)
+    perm = api.DeviceArray(ctx, n, np.uint32)
+    srt.sort(p, m, perm)
+    ref, ref_perm = orc.sort_by_cell(rec, n, met["heights"], (spec.nx, spec.ny, spec.nz))
+    assert np.array_equal(perm.numpy(), ref_perm)
+    assert np.array_equal(p.download(), ref)
+    # a partial dispatch range leaves the tail in place
+    p.upload(rec)
+    p.dispatch_count = n // 2
+    srt.sort(p, m)
+    ref2, _ = orc.sort_by_cell(rec, n // 2, met["heights"], (spec.nx, spec.ny, spec.nz))
+    assert np.array_equal(p.download(), ref2)
