@@ -1,0 +1,393 @@
+// driver.cu — the forward time loop (ForwardTimeLoopDriver,
+// src/simulation/timeloop.rs:660-1431) and the release manager
+// (src/release/mod.rs:55-275) as host C++ over the fpg.h entry points.
+//
+// Host bookkeeping mirrors ParticleStore (src/particles/mod.rs:477-605):
+// slots are handed out from the lowest free index; nothing on the device
+// deactivates a particle, so the free slots are always [next_free, capacity)
+// (after a compaction: [active_count, capacity), reset_after_compaction).
+//
+// Launch range and Philox counters: the reference dispatches every capacity
+// slot and advances the counter by dispatch_count * blocks per step
+// (gpu/langevin_fused.rs:229-233); slots at or above next_free are zeroed
+// (inactive) and their kernels return at once.  The driver launches only
+// [0, next_free) and advances the counter by the reference's dispatch count,
+// so every particle draws the same Philox blocks as in the reference.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/fpg_driver.h"
+#include "fpg_internal.h"
+
+namespace {
+
+struct ReleaseState {
+    fpg_release cfg;
+    uint64_t released = 0;
+    int32_t release_point = 0;
+};
+
+int64_t days_from_civil(int64_t y, int64_t m, int64_t d) {
+    if (m <= 2) y -= 1;
+    const int64_t era = (y >= 0 ? y : y - 399) / 400;
+    const int64_t yoe = y - era * 400;
+    const int64_t mp = m + (m > 2 ? -3 : 9);
+    const int64_t doy = (153 * mp + 2) / 5 + d - 1;
+    const int64_t doe = yoe * 365 + yoe / 4 - yoe / 100 + doy;
+    return era * 146097 + doe - 719468;
+}
+
+// ReleaseState::target_emitted_count (release/mod.rs:181-196).
+uint64_t target_emitted(const ReleaseState& s, int64_t now) {
+    const fpg_release& r = s.cfg;
+    if (now < r.start_seconds || now > r.end_seconds) return s.released;
+    if (r.start_seconds == r.end_seconds) return r.particle_count;
+    if (now == r.end_seconds) return r.particle_count;
+    const unsigned __int128 e = (uint64_t)(now - r.start_seconds);
+    const unsigned __int128 d = (uint64_t)(r.end_seconds - r.start_seconds);
+    return (uint64_t)(((unsigned __int128)r.particle_count * e) / d);
+}
+
+// ReleaseBounds::sample_stratified (release/mod.rs:256-275).
+void sample_stratified(const fpg_release& r, uint64_t index, uint64_t total, double& lon, double& lat, double& z) {
+    double c = std::ceil(std::cbrt((double)total));
+    if (c < 1.0) c = 1.0;
+    const uint64_t nx = (uint64_t)c, ny = nx;
+    uint64_t nxy = nx * ny;
+    if (nxy < 1) nxy = 1;
+    uint64_t nz = (total + nxy - 1) / nxy;
+    if (nz < 1) nz = 1;
+    const uint64_t ix = index % nx, iy = (index / nx) % ny, iz = (index / nxy) % nz;
+    const double fx = ((double)ix + 0.5) / (double)nx;
+    const double fy = ((double)iy + 0.5) / (double)ny;
+    const double fz = ((double)iz + 0.5) / (double)nz;
+    lon = r.lon_min + fx * (r.lon_max - r.lon_min);
+    lat = r.lat_min + fy * (r.lat_max - r.lat_min);
+    z = r.z_min + fz * (r.z_max - r.z_min);
+}
+
+}  // namespace
+
+struct fpg_forward {
+    fpg_ctx* ctx = nullptr;
+    fpg_forward_config cfg{};
+    fpg_grid_domain domain{};
+    std::vector<ReleaseState> releases;
+    size_t capacity = 0;
+    fpg_particles* particles = nullptr;
+    fpg_met* met = nullptr;
+    fpg_surface* surface = nullptr;
+    fpg_pbl* pbl = nullptr;
+    fpg_compaction* compaction = nullptr;
+    fpg_sorter* sorter = nullptr;
+    int64_t t = 0;
+    uint64_t step_index = 0;
+    uint32_t counter[4] = {0, 0, 0, 0};
+    size_t next_free = 0;
+    size_t active = 0;
+    bool have_bracket = false;
+    int64_t bracket_t0 = 0, bracket_t1 = 0;
+    float* d_forcing[3] = {nullptr, nullptr, nullptr};   // dry velocity, wet lambda, wet fraction per slot
+    std::vector<fpg_particle> staging;
+};
+
+using namespace fpg;
+
+extern "C" void fpg_forward_config_default(fpg_forward_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->start_seconds = 1704067200;   // 20240101000000
+    c->end_seconds = 1704067200;
+    c->timestep_seconds = 1;
+    c->clamp_time_bounds = 1;
+    c->x_grid_per_meter = c->y_grid_per_meter = c->z_grid_per_meter = 1.0f;
+    c->pbl_options = fpg_pbl_options{0.1f, 10.0f, 1.0f, 800.0f, 100.0f, 4500.0f};
+    c->dry_reference_height_m = 15.0f;
+    c->philox_key[0] = 0xDECAFBADu;
+    c->philox_key[1] = 0x12345678u;
+    c->sort_interval_steps = 0;
+    c->use_compaction = 0;
+    c->n_substeps = 4;
+    c->min_height_m = 0.01f;
+}
+
+extern "C" fpg_status fpg_parse_timestamp(const char* s, int64_t* out) {
+    if (!s || !out || std::strlen(s) != 14) return FPG_ERR_INVALID_ARGUMENT;
+    int v[14];
+    for (int i = 0; i < 14; ++i) {
+        if (s[i] < '0' || s[i] > '9') return FPG_ERR_INVALID_ARGUMENT;
+        v[i] = s[i] - '0';
+    }
+    const int64_t year = v[0] * 1000 + v[1] * 100 + v[2] * 10 + v[3];
+    const int64_t month = v[4] * 10 + v[5], day = v[6] * 10 + v[7];
+    const int64_t hour = v[8] * 10 + v[9], minute = v[10] * 10 + v[11], second = v[12] * 10 + v[13];
+    if (month < 1 || month > 12 || day < 1 || day > 31 || hour > 23 || minute > 59 || second > 59)
+        return FPG_ERR_INVALID_ARGUMENT;
+    *out = days_from_civil(year, month, day) * 86400 + hour * 3600 + minute * 60 + second;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_destroy(fpg_forward* d) {
+    if (!d) return FPG_OK;
+    fpg_ctx_synchronize(d->ctx, nullptr);
+    fpg_particles_destroy(d->particles);
+    fpg_met_destroy(d->met);
+    fpg_surface_destroy(d->surface);
+    fpg_pbl_destroy(d->pbl);
+    fpg_compaction_destroy(d->compaction);
+    fpg_sorter_destroy(d->sorter);
+    for (float* p : d->d_forcing) cudaFree(p);
+    delete d;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_create(fpg_ctx* ctx, const fpg_forward_config* cfg, const fpg_release* rel,
+                                         size_t n_rel, const fpg_grid_domain* grid, size_t capacity, size_t nx,
+                                         size_t ny, size_t nz, const float* heights, fpg_forward** out) {
+    if (!ctx || !cfg || !grid || !out || (n_rel && !rel)) return FPG_ERR_INVALID_ARGUMENT;
+    // validate_config (timeloop.rs:1932-1972)
+    if (cfg->start_seconds > cfg->end_seconds) return FPG_ERR_INVALID_TIME_RANGE;
+    if (cfg->timestep_seconds <= 0) return FPG_ERR_INVALID_TIME_STEP;
+    if (!std::isfinite(cfg->dry_reference_height_m) || cfg->dry_reference_height_m <= 0.0f)
+        return FPG_ERR_INVALID_REFERENCE_HEIGHT;
+    // ReleaseBounds::from_config (release/mod.rs:221-244)
+    for (size_t i = 0; i < n_rel; ++i)
+        if (rel[i].lon_min > rel[i].lon_max || rel[i].lat_min > rel[i].lat_max || rel[i].z_min > rel[i].z_max)
+            return FPG_ERR_INVALID_BOUNDS;
+    fpg_forward* d = new fpg_forward();
+    d->ctx = ctx;
+    d->cfg = *cfg;
+    d->domain = *grid;
+    d->capacity = capacity;
+    d->t = cfg->start_seconds;
+    std::memcpy(d->counter, cfg->initial_philox_counter, sizeof(d->counter));
+    for (size_t i = 0; i < n_rel; ++i) {
+        ReleaseState s;
+        s.cfg = rel[i];
+        s.release_point = (int32_t)i;
+        d->releases.push_back(s);
+    }
+    fpg_status st = fpg_particles_create(ctx, capacity, &d->particles);
+    if (st == FPG_OK) st = fpg_met_create(ctx, nx, ny, nz, &d->met);
+    if (st == FPG_OK && heights) st = fpg_met_set_level_heights(d->met, heights, nz);
+    if (st == FPG_OK) st = fpg_surface_create(ctx, nx, ny, &d->surface);
+    if (st == FPG_OK) st = fpg_pbl_create(ctx, nx, ny, &d->pbl);
+    if (st == FPG_OK && cfg->use_compaction) st = fpg_compaction_create(ctx, capacity, &d->compaction);
+    if (st == FPG_OK && cfg->sort_interval_steps) st = fpg_sorter_create(ctx, capacity, &d->sorter);
+    if (st != FPG_OK) {
+        fpg_forward_destroy(d);
+        return st;
+    }
+    *out = d;
+    return FPG_OK;
+}
+
+extern "C" int32_t fpg_forward_has_remaining_steps(const fpg_forward* d) { return d && d->t <= d->cfg.end_seconds; }
+extern "C" int64_t fpg_forward_current_time(const fpg_forward* d) { return d ? d->t : 0; }
+extern "C" fpg_particles* fpg_forward_particles(fpg_forward* d) { return d ? d->particles : nullptr; }
+
+extern "C" fpg_status fpg_forward_finalize(fpg_forward* d) {
+    if (!d) return FPG_ERR_INVALID_ARGUMENT;
+    return fpg_ctx_synchronize(d->ctx, nullptr);
+}
+
+// ReleaseManager::inject_for_time + upload of the touched slots
+// (release/mod.rs:90-168).
+static fpg_status release_for_time(fpg_forward* d, int64_t now, uint64_t& released, uint64_t& first_slot) {
+    released = 0;
+    first_slot = d->next_free;
+    d->staging.clear();
+    for (ReleaseState& s : d->releases) {
+        const uint64_t target = target_emitted(s, now);
+        if (target <= s.released) continue;
+        const uint64_t to_emit = target - s.released;
+        const float mass_per_particle = (float)(s.cfg.mass_kg / (double)s.cfg.particle_count);
+        for (uint64_t k = 0; k < to_emit; ++k) {
+            double lon, lat, z;
+            sample_stratified(s.cfg, s.released + k, s.cfg.particle_count, lon, lat, z);
+            // geo_to_grid, GridDomain::contains, GridCoord::to_relative (coords/mod.rs:92-114,169-178)
+            const double x = (lon - d->domain.xlon0) / d->domain.dx;
+            const double y = (lat - d->domain.ylat0) / d->domain.dy;
+            if (!(x >= 0.0 && x < (double)(d->domain.nx - 1) && y >= 0.0 && y < (double)(d->domain.ny - 1)))
+                return FPG_ERR_OUT_OF_GRID;
+            if (d->next_free + d->staging.size() >= d->capacity) return FPG_ERR_STORE_FULL;
+            const double fx = std::floor(x), fy = std::floor(y);
+            fpg_particle p;
+            std::memset(&p, 0, sizeof(p));
+            p.cell_x = (int32_t)fx;
+            p.cell_y = (int32_t)fy;
+            p.pos_x = (float)(x - fx);
+            p.pos_y = (float)(y - fy);
+            p.pos_z = (float)z;
+            p.flags = FPG_FLAG_ACTIVE;
+            p.mass[0] = mass_per_particle;
+            p.time = (int32_t)now;
+            p.time_mem = (int32_t)now;
+            p.release_point = s.release_point;
+            d->staging.push_back(p);
+        }
+        s.released = target;
+    }
+    if (d->staging.empty()) return FPG_OK;
+    const fpg_status st = fpg_particles_upload(d->particles, d->next_free, d->staging.size(), d->staging.data(),
+                                               nullptr);
+    if (st != FPG_OK) return st;
+    released = d->staging.size();
+    d->next_free += released;
+    d->active += released;
+    return FPG_OK;
+}
+
+static fpg_status upload_forcing(fpg_forward* d, int k, const float* host) {
+    if (!d->d_forcing[k]) FPG_CUDA(cudaMalloc(&d->d_forcing[k], (d->capacity > 0 ? d->capacity : 1) * sizeof(float)));
+    FPG_CUDA(cudaMemcpyAsync(d->d_forcing[k], host, d->capacity * sizeof(float), cudaMemcpyHostToDevice,
+                             d->ctx->stream));
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bracket* met, const fpg_forcing* f,
+                                               fpg_step_report* report) {
+    if (!d || !met || !f) return FPG_ERR_INVALID_ARGUMENT;
+    if (!fpg_forward_has_remaining_steps(d)) return FPG_ERR_SIMULATION_COMPLETE;
+    fpg_status st;
+
+    // apply_spatial_sort_if_enabled (timeloop.rs:1414-1430)
+    if (d->sorter && d->step_index % d->cfg.sort_interval_steps == 0 && d->next_free > 0) {
+        const size_t keep = d->particles->dispatch;
+        d->particles->dispatch = d->next_free;
+        st = fpg_sort_by_cell(d->ctx, d->particles, d->met, d->sorter, nullptr, nullptr);
+        d->particles->dispatch = keep;
+        if (st != FPG_OK) return st;
+    }
+
+    uint64_t released = 0, first_slot = 0;
+    st = release_for_time(d, d->t, released, first_slot);
+    if (st != FPG_OK) return st;
+
+    // interpolation_alpha (timeloop.rs:2086-2120)
+    const int64_t t0 = met->time_t0_seconds, t1 = met->time_t1_seconds;
+    if (t1 <= t0) return FPG_ERR_INVALID_BRACKET;
+    int64_t eff = d->t;
+    if (!(d->t >= t0 && d->t <= t1)) {
+        if (!d->cfg.clamp_time_bounds) return FPG_ERR_OUTSIDE_BRACKET;
+        eff = d->t < t0 ? t0 : t1;
+    }
+    const float alpha = (float)((double)(eff - t0) / (double)(t1 - t0));
+
+    // upload_dual_wind_if_bracket_changed (timeloop.rs:1378-1402) + surface frames
+    if (!d->have_bracket || d->bracket_t0 != t0 || d->bracket_t1 != t1) {
+        if (!met->wind_t0_u || !met->wind_t0_v || !met->wind_t0_w || !met->wind_t1_u || !met->wind_t1_v ||
+            !met->wind_t1_w || !met->surface_t0 || !met->surface_t1)
+            return FPG_ERR_INVALID_ARGUMENT;
+        if ((st = fpg_met_upload_frame(d->met, 0, met->wind_t0_u, met->wind_t0_v, met->wind_t0_w, nullptr))) return st;
+        if ((st = fpg_met_upload_frame(d->met, 1, met->wind_t1_u, met->wind_t1_v, met->wind_t1_w, nullptr))) return st;
+        if ((st = fpg_surface_upload(d->surface, 0, met->surface_t0, nullptr))) return st;
+        if ((st = fpg_surface_upload(d->surface, 1, met->surface_t1, nullptr))) return st;
+        d->have_bracket = true;
+        d->bracket_t0 = t0;
+        d->bracket_t1 = t1;
+    }
+    // interpolate_surface_fields_linear + encode_pbl_diagnostics (timeloop.rs:961-988,1079-1088)
+    if ((st = fpg_pbl_diagnostics(d->ctx, d->surface, alpha, &d->cfg.pbl_options, d->pbl, nullptr))) return st;
+
+    // the fused step (timeloop.rs:1095-1180)
+    const float dt = (float)d->cfg.timestep_seconds;
+    fpg_step_params p;
+    fpg_step_params_default(&p);
+    p.alpha = alpha;
+    p.dt_seconds = dt;
+    p.turb_dt_seconds = dt;
+    p.x_grid_per_meter = d->cfg.x_grid_per_meter;
+    p.y_grid_per_meter = d->cfg.y_grid_per_meter;
+    p.z_grid_per_meter = d->cfg.z_grid_per_meter;
+    p.n_substeps = d->cfg.n_substeps;
+    p.min_height_m = d->cfg.min_height_m;
+    p.rho_grad_over_rho = f->rho_grad_over_rho;
+    p.key[0] = d->cfg.philox_key[0];
+    p.key[1] = d->cfg.philox_key[1];
+    std::memcpy(p.counter, d->counter, sizeof(p.counter));
+    p.dry_reference_height_m = d->cfg.dry_reference_height_m;
+    // is_zero(): Uniform(0) skips the process (timeloop.rs:998-1000)
+    p.dry_mode = (f->dry_mode == FPG_FORCING_UNIFORM && f->dry_velocity_m_s == 0.0f) ? FPG_FORCING_NONE : f->dry_mode;
+    p.dry_velocity_m_s = f->dry_velocity_m_s;
+    if (p.dry_mode == FPG_FORCING_PER_PARTICLE) {
+        if (!f->dry_velocity_per_slot) return FPG_ERR_INVALID_ARGUMENT;
+        if ((st = upload_forcing(d, 0, f->dry_velocity_per_slot))) return st;
+        p.dry_velocity_dev = d->d_forcing[0];
+    }
+    const bool wet_zero = f->wet_mode == FPG_FORCING_UNIFORM && f->wet_lambda_s_inv == 0.0f && f->wet_fraction == 0.0f;
+    p.wet_mode = wet_zero ? FPG_FORCING_NONE : f->wet_mode;
+    p.wet_lambda_s_inv = f->wet_lambda_s_inv;
+    p.wet_fraction = f->wet_fraction;
+    if (p.wet_mode == FPG_FORCING_PER_PARTICLE) {
+        if (!f->wet_lambda_per_slot || !f->wet_fraction_per_slot) return FPG_ERR_INVALID_ARGUMENT;
+        if ((st = upload_forcing(d, 1, f->wet_lambda_per_slot))) return st;
+        if ((st = upload_forcing(d, 2, f->wet_fraction_per_slot))) return st;
+        p.wet_lambda_dev = d->d_forcing[1];
+        p.wet_fraction_dev = d->d_forcing[2];
+    }
+    p.wet_cells = f->wet_cells;
+
+    // The reference dispatches `dispatch` slots (capacity, or the active
+    // count with compaction); only [0, next_free) can hold particles.
+    const size_t ref_dispatch = d->compaction ? d->active : d->capacity;
+    d->particles->dispatch = d->next_free;
+    uint32_t ignored[4];
+    st = fpg_step(d->ctx, d->particles, d->met, d->pbl, &p, ignored, nullptr);
+    d->particles->dispatch = ref_dispatch;
+    if (st != FPG_OK) return st;
+    if (ref_dispatch > 0) {
+        // gpu/langevin_fused.rs:229-233
+        const uint64_t bpp = d->cfg.n_substeps <= 2u ? 1u : 2u;
+        const uint64_t off = (uint64_t)ref_dispatch * bpp;
+        const uint32_t lo = (uint32_t)off, hi = (uint32_t)(off >> 32);
+        uint32_t c0 = d->counter[0] + lo;
+        const uint32_t carry0 = c0 < d->counter[0];
+        const uint32_t n1 = d->counter[1] + hi;
+        const uint32_t carry1a = n1 < d->counter[1];
+        const uint32_t c1 = n1 + carry0;
+        const uint32_t carry1b = c1 < n1;
+        const uint32_t c2 = d->counter[2] + (carry1a | carry1b);
+        const uint32_t carry2 = c2 < d->counter[2];
+        d->counter[0] = c0;
+        d->counter[1] = c1;
+        d->counter[2] = c2;
+        d->counter[3] = d->counter[3] + carry2;
+    }
+
+    // compaction (timeloop.rs:1185-1197,1249-1262)
+    if (d->compaction) {
+        uint32_t act = 0;
+        d->particles->dispatch = d->capacity;
+        if ((st = fpg_compact(d->ctx, d->particles, d->compaction, &act, nullptr, nullptr))) return st;
+        d->active = act;
+        d->next_free = act;                       // reset_after_compaction (particles/mod.rs:600-605)
+        d->particles->dispatch = act;
+    }
+
+    if (report) {
+        report->step_index = d->step_index;
+        report->simulation_time_seconds = d->t;
+        report->interpolation_alpha = alpha;
+        report->released_count = released;
+        report->first_released_slot = first_slot;
+        report->active_particle_count = d->active;
+        std::memcpy(report->next_philox_counter, d->counter, sizeof(d->counter));
+    }
+    d->step_index += 1;
+    d->t += d->cfg.timestep_seconds;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_accumulate_grid(fpg_forward* d, fpg_grid* grid, uint32_t species, float scale,
+                                                  const float* outheights, size_t n_oh) {
+    if (!d || !grid) return FPG_ERR_INVALID_ARGUMENT;
+    const size_t keep = d->particles->dispatch;
+    d->particles->dispatch = d->next_free;
+    const fpg_status st = fpg_grid_accumulate(d->ctx, d->particles, grid, species, scale, outheights, n_oh, nullptr);
+    d->particles->dispatch = keep;
+    return st;
+}

@@ -106,6 +106,16 @@ _sig("fpg_compaction_destroy", _i32, _vp)
 _sig("fpg_compact", _i32, _vp, _vp, _vp, _u32p, _vp, _vp)
 _sig("fpg_philox_uniforms", _i32, _vp, _u32p, _u32p, _sz, _vp, _vp, _vp)
 _sig("fpg_compaction_indices_static", _i32, _vp, _vp, _sz, _vp, _vp, _vp)
+_sig("fpg_forward_config_default", None, _vp)
+_sig("fpg_parse_timestamp", _i32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64))
+_sig("fpg_forward_create", _i32, _vp, _vp, _vp, _sz, _vp, _sz, _sz, _sz, _sz, _vp, ctypes.POINTER(_vp))
+_sig("fpg_forward_destroy", _i32, _vp)
+_sig("fpg_forward_has_remaining_steps", _i32, _vp)
+_sig("fpg_forward_current_time", ctypes.c_int64, _vp)
+_sig("fpg_forward_run_timestep", _i32, _vp, _vp, _vp, _vp)
+_sig("fpg_forward_finalize", _i32, _vp)
+_sig("fpg_forward_particles", _vp, _vp)
+_sig("fpg_forward_accumulate_grid", _i32, _vp, _vp, _u32, _f32, _vp, _sz)
 _sig("fpg_sorter_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
 _sig("fpg_sorter_destroy", _i32, _vp)
 _sig("fpg_sort_by_cell", _i32, _vp, _vp, _vp, _vp, _vp, _vp)
@@ -137,4 +147,11 @@ EXPORTED = [
     "fpg_philox_uniforms",
     "fpg_compaction_indices_static",
     "fpg_sorter_create", "fpg_sorter_destroy", "fpg_sort_by_cell",
+]
+
+# Every symbol include/fpg_driver.h declares.
+EXPORTED_DRIVER = [
+    "fpg_forward_config_default", "fpg_forward_create", "fpg_forward_destroy", "fpg_forward_has_remaining_steps",
+    "fpg_forward_current_time", "fpg_forward_run_timestep", "fpg_forward_finalize", "fpg_forward_particles",
+    "fpg_forward_accumulate_grid", "fpg_parse_timestamp",
 ]

@@ -95,9 +95,11 @@ class DeviceArray:
         return out
 
     def free(self):
-        if self.ptr:
+        # handles die before their context (include/fpg.h); a buffer collected
+        # after its context closed is left to the process exit
+        if self.ptr and self.ctx.h:
             lib.fpg_device_free(self.ctx.h, _vp(self.ptr))
-            self.ptr = None
+        self.ptr = None
 
     def __del__(self):
         try:
@@ -115,7 +117,7 @@ class Particles:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_particles_destroy(self.h)
         except Exception:
             pass
@@ -173,7 +175,7 @@ class Met:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_met_destroy(self.h)
         except Exception:
             pass
@@ -203,7 +205,7 @@ class Pbl:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_pbl_destroy(self.h)
         except Exception:
             pass
@@ -232,7 +234,7 @@ class Surface:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_surface_destroy(self.h)
         except Exception:
             pass
@@ -259,7 +261,7 @@ class CellField:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_cellfield_destroy(self.h)
         except Exception:
             pass
@@ -318,7 +320,7 @@ class Grid:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_grid_destroy(self.h)
         except Exception:
             pass
@@ -356,7 +358,7 @@ class Compaction:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_compaction_destroy(self.h)
         except Exception:
             pass
@@ -379,7 +381,7 @@ class Sorter:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and self.ctx.h:
                 lib.fpg_sorter_destroy(self.h)
         except Exception:
             pass

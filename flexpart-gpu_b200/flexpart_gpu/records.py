@@ -135,6 +135,77 @@ class PblOptions(ctypes.Structure):
         return cls(0.1, 10.0, 1.0, 800.0, 100.0, 4500.0)
 
 
+class Release(ctypes.Structure):
+    """``fpg_release`` (include/fpg_driver.h): ReleaseConfig as the release
+    manager reads it (src/release/mod.rs:199-254)."""
+
+    _fields_ = [
+        ("start_seconds", ctypes.c_int64), ("end_seconds", ctypes.c_int64),
+        ("lon_min", ctypes.c_double), ("lon_max", ctypes.c_double),
+        ("lat_min", ctypes.c_double), ("lat_max", ctypes.c_double),
+        ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
+        ("mass_kg", ctypes.c_double), ("particle_count", ctypes.c_uint64),
+    ]
+
+
+class GridDomain(ctypes.Structure):
+    """``fpg_grid_domain``: GridDomain (src/coords/mod.rs)."""
+
+    _fields_ = [("xlon0", ctypes.c_double), ("ylat0", ctypes.c_double), ("dx", ctypes.c_double),
+                ("dy", ctypes.c_double), ("nx", ctypes.c_uint64), ("ny", ctypes.c_uint64)]
+
+
+class ForwardConfig(ctypes.Structure):
+    """``fpg_forward_config``: ForwardTimeLoopConfig (timeloop.rs:67-124)."""
+
+    _fields_ = [
+        ("start_seconds", ctypes.c_int64), ("end_seconds", ctypes.c_int64), ("timestep_seconds", ctypes.c_int64),
+        ("clamp_time_bounds", ctypes.c_int32),
+        ("x_grid_per_meter", ctypes.c_float), ("y_grid_per_meter", ctypes.c_float),
+        ("z_grid_per_meter", ctypes.c_float),
+        ("pbl_options", PblOptions),
+        ("dry_reference_height_m", ctypes.c_float),
+        ("philox_key", ctypes.c_uint32 * 2), ("initial_philox_counter", ctypes.c_uint32 * 4),
+        ("sort_interval_steps", ctypes.c_uint32), ("use_compaction", ctypes.c_int32),
+        ("n_substeps", ctypes.c_uint32), ("min_height_m", ctypes.c_float),
+    ]
+
+
+class MetBracket(ctypes.Structure):
+    """``fpg_met_bracket``: MetTimeBracket (timeloop.rs:270-285)."""
+
+    _fields_ = [
+        ("wind_t0_u", ctypes.c_void_p), ("wind_t0_v", ctypes.c_void_p), ("wind_t0_w", ctypes.c_void_p),
+        ("wind_t1_u", ctypes.c_void_p), ("wind_t1_v", ctypes.c_void_p), ("wind_t1_w", ctypes.c_void_p),
+        ("surface_t0", ctypes.c_void_p), ("surface_t1", ctypes.c_void_p),
+        ("time_t0_seconds", ctypes.c_int64), ("time_t1_seconds", ctypes.c_int64),
+    ]
+
+
+class Forcing(ctypes.Structure):
+    """``fpg_forcing``: ForwardStepForcing (timeloop.rs:347-358)."""
+
+    _fields_ = [
+        ("dry_mode", ctypes.c_int32), ("dry_velocity_m_s", ctypes.c_float),
+        ("dry_velocity_per_slot", ctypes.c_void_p),
+        ("wet_mode", ctypes.c_int32), ("wet_lambda_s_inv", ctypes.c_float), ("wet_fraction", ctypes.c_float),
+        ("wet_lambda_per_slot", ctypes.c_void_p), ("wet_fraction_per_slot", ctypes.c_void_p),
+        ("wet_cells", ctypes.c_void_p),
+        ("rho_grad_over_rho", ctypes.c_float),
+    ]
+
+
+class StepReport(ctypes.Structure):
+    """``fpg_step_report``: ForwardStepReport (timeloop.rs:1294-1308)."""
+
+    _fields_ = [
+        ("step_index", ctypes.c_uint64), ("simulation_time_seconds", ctypes.c_int64),
+        ("interpolation_alpha", ctypes.c_float), ("released_count", ctypes.c_uint64),
+        ("first_released_slot", ctypes.c_uint64), ("active_particle_count", ctypes.c_uint64),
+        ("next_philox_counter", ctypes.c_uint32 * 4),
+    ]
+
+
 def particles_from_soa(fields: dict, n: int) -> np.ndarray:
     """Builds fpg_particle records from a dict of per-field arrays."""
     rec = np.zeros(n, dtype=PARTICLE_DTYPE)

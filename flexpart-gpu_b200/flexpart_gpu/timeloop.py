@@ -1,0 +1,178 @@
+"""ForwardDriver: the forward time loop behind the C ABI (include/fpg_driver.h),
+in the shape of the reference's ForwardTimeLoopDriver
+(src/simulation/timeloop.rs:660-1431): ``run_timestep(met, forcing)``,
+``run_to_end``, ``has_remaining_steps``, ``finalize``,
+``accumulate_concentration_grid``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import synthetic
+from ._lib import check, lib
+from .api import Context, Grid, Particles
+from .records import (
+    FORCING_NONE,
+    FORCING_PER_CELL,
+    FORCING_UNIFORM,
+    ForwardConfig,
+    Forcing,
+    GridDomain,
+    MetBracket,
+    PblOptions,
+    Release,
+    StepReport,
+)
+
+_vp = ctypes.c_void_p
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class _ParticlesView(Particles):
+    """A Particles object over the driver's own handle (not owned)."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = _vp(handle)
+
+    def __del__(self):
+        pass
+
+
+class ForwardDriver:
+    def __init__(self, ctx: Context, config: ForwardConfig, releases, grid: GridDomain, capacity: int,
+                 met_shape, level_heights=None):
+        self.ctx = ctx
+        self.config = config
+        rel = (Release * max(len(releases), 1))(*releases)
+        nx, ny, nz = met_shape
+        self._heights = None if level_heights is None else np.ascontiguousarray(level_heights, np.float32)
+        h = _vp()
+        check(lib.fpg_forward_create(ctx.h, ctypes.byref(config), rel, len(releases), ctypes.byref(grid), capacity,
+                                     nx, ny, nz, _p(self._heights), ctypes.byref(h)), "fpg_forward_create")
+        self.h = h
+        self.capacity = capacity
+        self.met_shape = met_shape
+        self._keep = []
+
+    def __del__(self):
+        # the driver synchronises its context's stream when destroyed, so it
+        # must go before the context (include/fpg_driver.h)
+        try:
+            if self.h and self.ctx.h:
+                lib.fpg_forward_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def has_remaining_steps(self) -> bool:
+        return bool(lib.fpg_forward_has_remaining_steps(self.h))
+
+    @property
+    def current_time_seconds(self) -> int:
+        return int(lib.fpg_forward_current_time(self.h))
+
+    @property
+    def particles(self) -> Particles:
+        return _ParticlesView(self.ctx, lib.fpg_forward_particles(self.h))
+
+    def run_timestep(self, met: MetBracket, forcing: Forcing) -> StepReport:
+        rep = StepReport()
+        check(lib.fpg_forward_run_timestep(self.h, ctypes.byref(met), ctypes.byref(forcing), ctypes.byref(rep)),
+              "fpg_forward_run_timestep")
+        return rep
+
+    def finalize(self):
+        check(lib.fpg_forward_finalize(self.h), "fpg_forward_finalize")
+
+    def accumulate_concentration_grid(self, grid: Grid, species=0, mass_scale=1.0e6, outheights=None):
+        oh = None if outheights is None else np.ascontiguousarray(outheights, np.float32)
+        check(lib.fpg_forward_accumulate_grid(self.h, grid.h, species, mass_scale, _p(oh),
+                                              0 if oh is None else oh.size), "fpg_forward_accumulate_grid")
+        return grid.download()
+
+
+def default_config(**kw) -> ForwardConfig:
+    c = ForwardConfig()
+    lib.fpg_forward_config_default(ctypes.byref(c))
+    for k, v in kw.items():
+        if k in ("philox_key", "initial_philox_counter"):
+            arr = getattr(c, k)
+            for i, x in enumerate(v):
+                arr[i] = int(x) & 0xFFFFFFFF
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def parse_timestamp(s: str) -> int:
+    out = ctypes.c_int64()
+    check(lib.fpg_parse_timestamp(s.encode(), ctypes.byref(out)), "fpg_parse_timestamp")
+    return out.value
+
+
+# ---- scenario plumbing -----------------------------------------------------
+
+def scenario_releases(scn: synthetic.Scenario):
+    out = []
+    for s in scn.sources:
+        out.append(Release(s.start, s.end, s.lon, s.lon if s.lon_max is None else s.lon_max, s.lat,
+                           s.lat if s.lat_max is None else s.lat_max, s.z_min, s.z_max, s.mass_kg, s.particle_count))
+    return out
+
+
+def scenario_domain(scn: synthetic.Scenario) -> GridDomain:
+    m = scn.met
+    return GridDomain(m.xlon0, m.ylat0, m.dx_deg, m.dy_deg, m.nx, m.ny)
+
+
+def scenario_config(scn: synthetic.Scenario, **kw) -> ForwardConfig:
+    xs, ys, zs = synthetic.velocity_scale(scn.met)
+    base = dict(start_seconds=scn.start, end_seconds=scn.end, timestep_seconds=scn.dt, x_grid_per_meter=xs,
+                y_grid_per_meter=ys, z_grid_per_meter=zs, philox_key=scn.key)
+    base.update(kw)
+    return default_config(**base)
+
+
+class BracketSource:
+    """Builds the MetBracket of a scenario at time t from its frame ring
+    (host arrays kept alive here)."""
+
+    def __init__(self, scn: synthetic.Scenario, frames):
+        self.scn = scn
+        self.frames = [{k: np.ascontiguousarray(f[k].reshape(-1)) for k in ("u", "v", "w")} | {"surface": f["surface"]}
+                       for f in frames]
+
+    def at(self, t: int) -> MetBracket:
+        fa, fb, ta, tb = synthetic.bracket_frames(self.scn, t)
+        a, b = self.frames[fa], self.frames[fb]
+        return MetBracket(a["u"].ctypes.data, a["v"].ctypes.data, a["w"].ctypes.data, b["u"].ctypes.data,
+                          b["v"].ctypes.data, b["w"].ctypes.data, a["surface"].ctypes.data,
+                          b["surface"].ctypes.data, ta, tb)
+
+
+def uniform_forcing(dry_velocity=0.0, wet_lambda=0.0, wet_fraction=0.0, rho_grad_over_rho=0.0) -> Forcing:
+    f = Forcing()
+    f.dry_mode = FORCING_UNIFORM
+    f.dry_velocity_m_s = dry_velocity
+    f.wet_mode = FORCING_UNIFORM
+    f.wet_lambda_s_inv = wet_lambda
+    f.wet_fraction = wet_fraction
+    f.rho_grad_over_rho = rho_grad_over_rho
+    return f
+
+
+def cell_forcing(cells, dry_velocity=0.0, rho_grad_over_rho=0.0) -> Forcing:
+    f = uniform_forcing(dry_velocity, 0.0, 0.0, rho_grad_over_rho)
+    f.wet_mode = FORCING_PER_CELL
+    f.wet_cells = cells.h.value
+    return f
+
+
+__all__ = ["ForwardDriver", "default_config", "parse_timestamp", "scenario_releases", "scenario_domain",
+           "scenario_config", "BracketSource", "uniform_forcing", "cell_forcing", "FORCING_NONE", "PblOptions"]

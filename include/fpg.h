@@ -63,6 +63,7 @@ enum {
     FPG_ERR_INVALID_BOUNDS = -15,    /* ReleaseError::InvalidBounds: release/mod.rs:33 */
     FPG_ERR_OUT_OF_GRID = -16,       /* ReleaseError::OutOfGridDomain: release/mod.rs:41 */
     FPG_ERR_TOO_MANY_LEVELS = -17,   /* more than FPG_MAX_LEVELS heights */
+    FPG_ERR_INVALID_TIME_RANGE = -18, /* TimeLoopError::InvalidTimeRange: simulation/timeloop.rs:1935 */
     FPG_ERR_CUDA = -100,             /* any CUDA runtime error (see fpg_last_cuda_error) */
     FPG_ERR_OUT_OF_MEMORY = -101,
     FPG_ERR_NO_DEVICE = -102
@@ -125,6 +126,7 @@ typedef struct fpg_ctx fpg_ctx;
 
 /* GpuContext::new (src/gpu/mod.rs:163-208): binds `device`, creates a stream. */
 fpg_status fpg_ctx_create(int32_t device, fpg_ctx** out);
+/* Every handle created on a context must be destroyed before the context. */
 fpg_status fpg_ctx_destroy(fpg_ctx* ctx);
 /* The context's stream as a cudaStream_t. */
 void* fpg_ctx_stream(fpg_ctx* ctx);

@@ -1,0 +1,134 @@
+"""The forward time loop behind the C ABI (fpg_forward_*) against the oracle's
+forward loop: per-step reports (released counts, alpha, Philox counter,
+active count) bit-exact, particle state within the step tolerance on the
+first steps, and after the full 24 h run of the 100 k-particle configuration
+the gridded mass per cell within 1e-4 of the released mass (1 kg)."""
+import numpy as np
+import pytest
+
+from flexpart_gpu import synthetic
+from helpers import field_checks
+from oracle.forward import OracleForward
+
+pytestmark = pytest.mark.gpu
+
+api = pytest.importorskip("flexpart_gpu.api")
+tl = pytest.importorskip("flexpart_gpu.timeloop")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def _small(particles=20_000, hours=6):
+    scn = synthetic.config0()
+    scn.sources[0].particle_count = particles
+    scn.capacity = particles
+    scn.end = scn.start + hours * 3600
+    return scn
+
+
+def _driver(ctx, scn, **kw):
+    cfg = tl.scenario_config(scn, **kw)
+    return tl.ForwardDriver(ctx, cfg, tl.scenario_releases(scn), tl.scenario_domain(scn), scn.capacity,
+                            (scn.met.nx, scn.met.ny, scn.met.nz),
+                            synthetic.level_heights(scn.met.nz, scn.met.top_m))
+
+
+def _check_report(rep, orep):
+    assert rep.released_count == orep["released"]
+    assert rep.interpolation_alpha == np.float32(orep["alpha"])
+    assert list(rep.next_philox_counter) == orep["counter"]
+    assert rep.active_particle_count == orep["active"]
+
+
+@pytest.mark.parametrize("mode", ["plain", "compaction", "sort"])
+def test_driver_steps_match_oracle_loop(ctx, mode):
+    scn = _small()
+    frames = synthetic.make_frames(scn.met)
+    kw = {"use_compaction": 1} if mode == "compaction" else {"sort_interval_steps": 3} if mode == "sort" else {}
+    okw = {"use_compaction": True} if mode == "compaction" else {"sort_interval": 3} if mode == "sort" else {}
+    drv = _driver(ctx, scn, **kw)
+    fw = OracleForward(scn, scn.capacity, frames, **okw)
+    fw64 = OracleForward(scn, scn.capacity, frames, dtype=np.float64, **okw)
+    src = tl.BracketSource(scn, frames)
+    forcing = tl.uniform_forcing(dry_velocity=0.002)
+    for k in range(8):
+        z_prev = fw.records()["pos_z"]
+        rep = drv.run_timestep(src.at(drv.current_time_seconds), forcing)
+        orep = fw.run_timestep({"dry_velocity": 0.002})
+        fw64.run_timestep({"dry_velocity": 0.002})
+        _check_report(rep, orep)
+        if k < 3:
+            g = drv.particles.download()
+            o = fw.records()
+            # heights at the step start (release height for particles released this step)
+            z_in = np.where(z_prev == 0.0, o["pos_z"], z_prev)
+            for name, ok in field_checks(g, fw.state, z_in, fw64.state).items():
+                assert ok.all(), (mode, k, name, np.flatnonzero(~ok)[:5])
+            assert np.array_equal(g["flags"], o["flags"])
+            assert np.array_equal(g["release_point"], o["release_point"])
+            assert np.array_equal(g["time"], o["time"])
+
+
+def test_full_24h_run_gridded_mass_within_1e4_of_released(ctx):
+    scn = synthetic.config0()
+    frames = synthetic.make_frames(scn.met)
+    drv = _driver(ctx, scn)
+    src = tl.BracketSource(scn, frames)
+    forcing = tl.uniform_forcing(dry_velocity=scn.dry_velocity)
+    fw = OracleForward(scn, scn.capacity, frames)
+    fw64 = OracleForward(scn, scn.capacity, frames, dtype=np.float64)
+    steps = 0
+    while drv.has_remaining_steps:
+        rep = drv.run_timestep(src.at(drv.current_time_seconds), forcing)
+        orep = fw.run_timestep({"dry_velocity": scn.dry_velocity})
+        fw64.run_timestep({"dry_velocity": scn.dry_velocity})
+        _check_report(rep, orep)
+        steps += 1
+    drv.finalize()
+    assert steps == 97 and not fw.has_remaining_steps
+    grid = api.Grid(ctx, *scn.out_shape)
+    counts, mass, kg = drv.accumulate_concentration_grid(grid, 0, 1e6, scn.outheights)
+    oc, om, _ = fw.grid()
+    oc64, om64, _ = fw64.grid()
+    released = sum(s.mass_kg for s in scn.sources)
+    d_gpu = np.abs(mass.astype(np.int64) - om.astype(np.int64)) / 1e6
+    d_fp32 = np.abs(om.astype(np.int64) - om64.astype(np.int64)) / 1e6
+    d_gpu64 = np.abs(mass.astype(np.int64) - om64.astype(np.int64)) / 1e6
+    print(f"24 h: max |mass_gpu - mass_oracle32| = {d_gpu.max():.2e} kg, vs FP64 {d_gpu64.max():.2e} kg; "
+          f"oracle32 vs FP64 {d_fp32.max():.2e} kg; counts differ by at most "
+          f"{np.abs(counts.astype(np.int64) - oc.astype(np.int64)).max()}")
+    assert counts.sum() == oc.sum() == 100_000
+    assert d_gpu.max() <= 1e-4 * released
+    assert d_gpu64.max() <= 1e-4 * released
+
+
+def test_driver_errors(ctx):
+    scn = _small(1000, 1)
+    with pytest.raises(api._lib.FpgError) as e:
+        tl.ForwardDriver(ctx, tl.scenario_config(scn, start_seconds=scn.end + 1), tl.scenario_releases(scn),
+                         tl.scenario_domain(scn), 1000, (scn.met.nx, scn.met.ny, scn.met.nz))
+    assert e.value.status == -18     # InvalidTimeRange (timeloop.rs:1935)
+    with pytest.raises(api._lib.FpgError) as e:
+        tl.ForwardDriver(ctx, tl.scenario_config(scn, timestep_seconds=0), tl.scenario_releases(scn),
+                         tl.scenario_domain(scn), 1000, (scn.met.nx, scn.met.ny, scn.met.nz))
+    assert e.value.status == -2      # InvalidTimestep
+    drv = _driver(ctx, scn)
+    frames = synthetic.make_frames(scn.met)
+    src = tl.BracketSource(scn, frames)
+    while drv.has_remaining_steps:
+        drv.run_timestep(src.at(drv.current_time_seconds), tl.uniform_forcing())
+    with pytest.raises(api._lib.FpgError) as e:
+        drv.run_timestep(src.at(scn.end), tl.uniform_forcing())
+    assert e.value.status == -14     # SimulationComplete (timeloop.rs:921)
+    small = _small(1000, 1)
+    small.capacity = 500             # the release overflows the store
+    drv2 = _driver(ctx, small)
+    with pytest.raises(api._lib.FpgError) as e:
+        for _ in range(5):
+            drv2.run_timestep(src.at(drv2.current_time_seconds), tl.uniform_forcing())
+    assert e.value.status == -9      # StoreFull (particles/mod.rs:516)
