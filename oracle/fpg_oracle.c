@@ -311,3 +311,12 @@ void orc_wet_cell(float lsp_in, float convp_in, float cloud_cover, float a_in, f
     *lambda_out = lambda;
     *fraction_out = fraction;
 }
+
+/* orc_wet_cell over a grid of n cells (convp / cloud_cover may be NULL:
+ * 0 and 1). */
+void orc_wet_cells_grid(size_t n, const float* lsp, const float* convp, const float* cloud_cover, float a,
+                        float b, float* lambda_out, float* fraction_out) {
+    for (size_t c = 0; c < n; ++c)
+        orc_wet_cell(lsp[c], convp ? convp[c] : 0.0f, cloud_cover ? cloud_cover[c] : 1.0f, a, b, &lambda_out[c],
+                     &fraction_out[c]);
+}

@@ -308,13 +308,13 @@ def wet_cell(lsp, convp, cc, a, b):
 
 
 def wet_cells(lsp, convp, cc, a, b):
-    lsp = np.asarray(lsp, np.float32).ravel()
-    convp = np.asarray(convp, np.float32).ravel()
-    cc = np.asarray(cc, np.float32).ravel()
+    lsp = np.ascontiguousarray(lsp, np.float32).ravel()
+    convp = None if convp is None else np.ascontiguousarray(convp, np.float32).ravel()
+    cc = None if cc is None else np.ascontiguousarray(cc, np.float32).ravel()
     lam = np.zeros_like(lsp)
     fr = np.zeros_like(lsp)
-    for i in range(len(lsp)):
-        lam[i], fr[i] = wet_cell(lsp[i], convp[i], cc[i], a, b)
+    lib.orc_wet_cells_grid(ctypes.c_size_t(lsp.size), _ptr(lsp), _ptr(convp), _ptr(cc), ctypes.c_float(a),
+                           ctypes.c_float(b), _ptr(lam), _ptr(fr))
     return lam, fr
 
 
