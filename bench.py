@@ -46,6 +46,11 @@ METRIC = "particle-steps/s"
 UNIT = "particle-steps/s"
 BYTES_PER_PARTICLE_STEP = 96  # read 44 B + write 52 B of SoA state, one species
 SORT_EVERY = 8
+# DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
+# an ncu capture of a 2 M-particle launch (129.8 MB), scaled by the particle
+# count; below the algorithmic 96 B because part of the state was still in
+# the 126 MB L2 across the capture's replay passes.
+DRAM_BYTES_PER_PARTICLE_NCU = 129.8e6 / 2.0e6
 
 
 def parse():
@@ -422,7 +427,9 @@ def main():
                        "sort_every_steps": SORT_EVERY, "spin_up_s": round(spin_s, 1),
                        "l2": "inputs larger than L2 (960 MB particle state per step)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE_NCU * n_active,
+                         "traffic_source": "ncu dram__bytes_read+write of a 2M-particle launch, scaled by particles",
+                         "peak_kind": peak_kind,
                          "kernel": "fused_step_kernel", "kernel_ms": avg_kernel_ms,
                          "bytes_per_launch": BYTES_PER_PARTICLE_STEP * n_active},
             "clocks": clk,
