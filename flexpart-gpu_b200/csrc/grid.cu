@@ -14,6 +14,7 @@
 #include <cstring>
 
 #include "fpg_internal.h"
+#include "grid_core.cuh"
 
 namespace fpg {
 
@@ -25,26 +26,6 @@ struct GridArgs {
     float mass_scale;
     int meters;  // outheights[nz-1] > 0
 };
-
-// pos_z_to_level (concentration_gridding.wgsl:304-315).
-__device__ __forceinline__ uint32_t level_of(float z, const float* h, uint32_t nz, int meters) {
-    if (meters) {
-        for (uint32_t k = 0; k < nz; ++k)
-            if (z <= h[k]) return k;
-        return nz - 1u;
-    }
-    // u32(clamp(i32(floor(z)), 0, nz-1)); float->int conversion saturates
-    const int iz = (int)floorf(z);
-    return (uint32_t)min(max(iz, 0), (int)nz - 1);
-}
-
-// quantize_mass_to_u32 (concentration_gridding.wgsl:317-326).
-__device__ __forceinline__ uint32_t quantize(float m, float scale) {
-    if (m <= 0.0f) return 0u;
-    const float scaled = m * scale + 0.5f;
-    if (scaled >= 4294967295.0f) return 0xffffffffu;
-    return (uint32_t)scaled;
-}
 
 __device__ __forceinline__ uint32_t cell_of(const GridArgs& a, const float* h, uint32_t p) {
     const int32_t cx = a.cell_x[p], cy = a.cell_y[p];

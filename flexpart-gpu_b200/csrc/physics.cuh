@@ -70,9 +70,13 @@ __device__ __forceinline__ float2 box_muller(float u0, float u1) {
 }
 
 // ---- Hanna (physics/hanna.rs:49-163, langevin_fused.wgsl:224-293) ----------
+// Stability branch of hanna.rs:69-112: 0 neutral, 1 unstable, 2 stable.
+enum { REGIME_NEUTRAL = 0, REGIME_UNSTABLE = 1, REGIME_STABLE = 2 };
+
 struct Hanna {
     float ust, wst, ol, h;
     float sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
+    int regime;
 };
 
 __device__ __forceinline__ float obukhov_from_inverse(float oli) {
@@ -88,7 +92,10 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
     const float z = clampf(z_in, 0.0f, h);
     const float zeta = clampf(z / h, 0.0f, 1.0f);
     float sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
-    if (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) {
+    o.regime = (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) ? REGIME_NEUTRAL
+               : ol < 0.0f                                         ? REGIME_UNSTABLE
+                                                                   : REGIME_STABLE;
+    if (o.regime == REGIME_NEUTRAL) {
         const float corr = z / ust;
         sigu = 1.0e-2f + 2.0f * ust * expf(-3.0e-4f * corr);
         sigw = 1.3f * ust * expf(-2.0e-4f * corr);
@@ -98,7 +105,7 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
         tlu = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
         tlv = tlu;
         tlw = tlu;
-    } else if (ol < 0.0f) {
+    } else if (o.regime == REGIME_UNSTABLE) {
         sigu = 1.0e-2f + ust * pow_third(12.0f - 0.5f * h / ol);
         sigv = sigu;
         const float c = pow_third(zeta);
@@ -140,21 +147,24 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
 
 // hanna_short_w (langevin_fused.wgsl:296-344): sigw, dsigwdz, tlw at a new
 // height.  ust, wst, h are the already-floored values of compute_hanna.
+// The branch test of the shader (`!finite(ol) || ol == 0 || h/|ol| < 1`,
+// then `ol < 0`) sees the same floored h and the same ol as compute_hanna's
+// for this particle, so its outcome is the `regime` compute_hanna found.
 __device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float ol, float h_in, float z_in,
-                                              float& sigw_o, float& dsigwdz_o, float& tlw_o) {
+                                              int regime, float& sigw_o, float& dsigwdz_o, float& tlw_o) {
     const float ust = fmaxf(ust_in, 1.0e-4f);
     const float wst = fmaxf(wst_in, 0.0f);
     const float h = fmaxf(h_in, 1.0f);
     const float z = clampf(z_in, 0.0f, h);
     const float zeta = clampf(z / h, 0.0f, 1.0f);
     float sigw, dsigwdz, tlw;
-    if (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) {
+    if (regime == REGIME_NEUTRAL) {
         const float corr = z / ust;
         sigw = 1.3f * ust * expf(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
         tlw = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
-    } else if (ol < 0.0f) {
+    } else if (regime == REGIME_UNSTABLE) {
         const float c = pow_third(zeta);
         const float z23 = c * c;
         const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
@@ -177,11 +187,13 @@ __device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float 
     sigw_o = sigw; dsigwdz_o = dsigwdz; tlw_o = tlw;
 }
 
+// The Langevin updates below take Hanna outputs only: sigma >= 0.01 and
+// T_L >= 10 s (30 s vertical), both finite after the clamps above, so the
+// reference's sanitize_positive() and its T_L == 0 return
+// (physics/langevin.rs:116-121,146-150) are the identity and are omitted.
+
 // ---- Langevin OU updates (physics/langevin.rs:116-170, langevin_fused.wgsl:350-389)
-__device__ __forceinline__ float langevin_h(float prev, float sigma_in, float tl_in, float dt, float eta) {
-    const float sigma = sanitize_positive(sigma_in);
-    const float tl = sanitize_positive(tl_in);
-    if (tl == 0.0f) return 0.0f;
+__device__ __forceinline__ float langevin_h(float prev, float sigma, float tl, float dt, float eta) {
     const float ratio = dt / tl;
     float next;
     if (ratio < 0.5f) {
@@ -193,11 +205,8 @@ __device__ __forceinline__ float langevin_h(float prev, float sigma_in, float tl
     return finitef(next) ? next : 0.0f;
 }
 
-__device__ __forceinline__ float langevin_v(float prev, float sigw_in, float tlw_in, float dsigwdz, float dt,
+__device__ __forceinline__ float langevin_v(float prev, float sigma_w, float tlw, float dsigwdz, float dt,
                                             float rho, float eta) {
-    const float sigma_w = sanitize_positive(sigw_in);
-    const float tlw = sanitize_positive(tlw_in);
-    if (tlw == 0.0f) return 0.0f;
     const float drift = sigma_w * (dsigwdz + rho * sigma_w);
     const float ratio = dt / tlw;
     float next;

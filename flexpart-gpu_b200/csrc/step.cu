@@ -30,142 +30,9 @@
 
 #include "fpg_internal.h"
 #include "physics.cuh"
+#include "step_core.cuh"
 
 namespace fpg {
-
-struct StepArgs {
-    int32_t* cell_x; int32_t* cell_y;
-    float* pos_x; float* pos_y; float* pos_z;
-    const uint32_t* flags;
-    float* mass[4];
-    float* vel_u; float* vel_v; float* vel_w;
-    float* turb_u; float* turb_v; float* turb_w;
-    int32_t* cbt;
-    uint32_t n;
-    int n_species;
-    uint32_t stages;
-    // advection
-    const float4* bracket;
-    const float* heights;
-    uint32_t nx, ny, nz;
-    int has_heights, monotonic;
-    float alpha, dt, xs, ys, zs;
-    // turbulence
-    const float4* pbl;
-    uint32_t pnx, pny;
-    float tdt, rho, zmin;
-    uint32_t n_sub;
-    uint32_t key0, key1;
-    u32x4 counter;
-    // deposition
-    float href;
-    int dry_mode;
-    float dry_v;
-    const float* dry_v_arr;
-    float* dry_prob;
-    int wet_mode;
-    float wet_l, wet_f;
-    const float* wet_l_arr;
-    const float* wet_f_arr;
-    const float2* wet_cells;
-    uint32_t wnx, wny;
-    float* wet_prob;
-};
-
-// meters_to_grid_level (advection_dual_wind.wgsl:94-117).
-__device__ __forceinline__ float meters_to_level(const float* h, uint32_t nz, int has, int mono, float z) {
-    if (!has) return z;
-    const float h0 = h[0];
-    if (z <= h0) return h0 > 0.0f ? z / h0 : 0.0f;
-    uint32_t k;
-    if (mono) {
-        // first k in [1, nz) with z <= h[k]; nz if none
-        uint32_t lo = 1u, hi = nz;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (z <= h[mid]) hi = mid; else lo = mid + 1u;
-        }
-        k = lo;
-    } else {
-        k = nz;
-        for (uint32_t i = 1u; i < nz; ++i) if (z <= h[i]) { k = i; break; }
-    }
-    if (k >= nz) return (float)(nz - 1u);
-    const float hprev = h[k - 1u];
-    const float denom = h[k] - hprev;
-    if (denom > 0.0f) return (float)(k - 1u) + (z - hprev) / denom;
-    return (float)(k - 1u);
-}
-
-// clamp_axis (advection_dual_wind.wgsl:130-138).
-__device__ __forceinline__ void axis_bracket(float coord, uint32_t n, uint32_t& lo, uint32_t& hi, float& t) {
-    const float c = clampf(coord, 0.0f, (float)(n - 1u));
-    const float lf = floorf(c);
-    lo = (uint32_t)lf;
-    hi = min(lo + 1u, n - 1u);
-    t = c - lf;
-}
-
-// sample_dual_{u,v,w} (advection_dual_wind.wgsl:142-236): trilinear in each
-// frame, then lerp by alpha.  The x-lerps of one (y, z) corner pair are taken
-// as soon as its four float4 (2 nodes x 2 frames) arrive, which keeps the
-// live registers at 16 floats instead of 64 while giving the same roundings
-// in the same order as the reference expression.
-struct Lerp6 { float u0, v0, w0, u1, v1, w1; };
-
-// One bracket node (t0 u,v,w,0 | t1 u,v,w,0) is 32 bytes at a 32-byte
-// aligned offset (cudaMalloc base, node stride 32 B): one 256-bit load.
-struct Node { float u0, v0, w0, p0, u1, v1, w1, p1; };
-
-__device__ __forceinline__ Node ld_node(const float4* br, uint32_t n) {
-    Node v;
-    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-        : "=f"(v.u0), "=f"(v.v0), "=f"(v.w0), "=f"(v.p0), "=f"(v.u1), "=f"(v.v1), "=f"(v.w1), "=f"(v.p1)
-        : "l"(br + 2u * n));
-    return v;
-}
-
-__device__ __forceinline__ Lerp6 xpair(const float4* br, uint32_t na, uint32_t nb, float tx) {
-    const Node a = ld_node(br, na);
-    const Node b = ld_node(br, nb);
-    return Lerp6{lerpf(a.u0, b.u0, tx), lerpf(a.v0, b.v0, tx), lerpf(a.w0, b.w0, tx),
-                 lerpf(a.u1, b.u1, tx), lerpf(a.v1, b.v1, tx), lerpf(a.w1, b.w1, tx)};
-}
-
-__device__ __forceinline__ Lerp6 lerp6(const Lerp6& a, const Lerp6& b, float t) {
-    return Lerp6{lerpf(a.u0, b.u0, t), lerpf(a.v0, b.v0, t), lerpf(a.w0, b.w0, t),
-                 lerpf(a.u1, b.u1, t), lerpf(a.v1, b.v1, t), lerpf(a.w1, b.w1, t)};
-}
-
-__device__ __forceinline__ float3 sample_dual(const StepArgs& a, const float* hts, float x, float y, float z) {
-    uint32_t x0, x1, y0, y1, z0, z1;
-    float tx, ty, tz;
-    axis_bracket(x, a.nx, x0, x1, tx);
-    axis_bracket(y, a.ny, y0, y1, ty);
-    axis_bracket(meters_to_level(hts, a.nz, a.has_heights, a.monotonic, z), a.nz, z0, z1, tz);
-    const uint32_t c00 = (x0 * a.ny + y0) * a.nz, c10 = (x1 * a.ny + y0) * a.nz;
-    const uint32_t c01 = (x0 * a.ny + y1) * a.nz, c11 = (x1 * a.ny + y1) * a.nz;
-    const float4* br = a.bracket;
-    // lerp(lerp(lerp(c000,c100,tx), lerp(c010,c110,tx), ty), lerp(lerp(c001,c101,tx), lerp(c011,c111,tx), ty), tz)
-    const Lerp6 l00 = xpair(br, c00 + z0, c10 + z0, tx);
-    const Lerp6 l10 = xpair(br, c01 + z0, c11 + z0, tx);
-    const Lerp6 l0 = lerp6(l00, l10, ty);
-    const Lerp6 l01 = xpair(br, c00 + z1, c10 + z1, tx);
-    const Lerp6 l11 = xpair(br, c01 + z1, c11 + z1, tx);
-    const Lerp6 l1 = lerp6(l01, l11, ty);
-    const Lerp6 t = lerp6(l0, l1, tz);
-    return make_float3(lerpf(t.u0, t.u1, a.alpha), lerpf(t.v0, t.v1, a.alpha), lerpf(t.w0, t.w1, a.alpha));
-}
-
-// split_horizontal_coord (advection_dual_wind.wgsl:238-248).
-__device__ __forceinline__ void split_coord(float coord, uint32_t n, int32_t& cell, float& frac) {
-    const float c = clampf(coord, 0.0f, (float)(n - 1u));
-    uint32_t ci = (uint32_t)floorf(c);
-    float f = c - (float)ci;
-    if (ci >= n - 1u) { ci = n - 1u; f = 0.0f; }
-    cell = (int32_t)ci;
-    frac = f;
-}
 
 __global__ void __launch_bounds__(256, 4) fused_step_kernel(StepArgs a) {
     extern __shared__ float s_heights[];
@@ -175,145 +42,11 @@ __global__ void __launch_bounds__(256, 4) fused_step_kernel(StepArgs a) {
     }
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
-    const bool dry_on = (a.stages & FPG_STAGE_DRY) && a.dry_mode != FPG_FORCING_NONE;
-    const bool wet_on = (a.stages & FPG_STAGE_WET) && a.wet_mode != FPG_FORCING_NONE;
-    if (!(a.flags[p] & FLAG_ACTIVE)) {
-        if (dry_on && a.dry_prob) a.dry_prob[p] = 0.0f;
-        if (wet_on && a.wet_prob) a.wet_prob[p] = 0.0f;
-        return;
-    }
-    int32_t cx = a.cell_x[p], cy = a.cell_y[p];
-    float px = a.pos_x[p], py = a.pos_y[p], pz = a.pos_z[p];
-    const bool turb_on = (a.stages & FPG_STAGE_TURBULENCE) != 0;
-    float tu = a.turb_u[p], tv = a.turb_v[p];
-
-    // ---- advection_dual_wind.wgsl:266-300 ----
-    if (a.stages & FPG_STAGE_ADVECT) {
-        const float x0 = (float)cx + px;
-        const float y0 = (float)cy + py;
-        const float z0 = pz;
-        const float3 s0 = sample_dual(a, s_heights, x0, y0, z0);
-        const float u0 = s0.x + tu, v0 = s0.y + tv, w0 = s0.z;
-        const float xmax = (float)(a.nx - 1u), ymax = (float)(a.ny - 1u);
-        const float ztop = a.has_heights ? s_heights[a.nz - 1u] : (float)(a.nz - 1u);
-        const float pxp = clampf(x0 + (u0 * a.xs) * a.dt, 0.0f, xmax);
-        const float pyp = clampf(y0 + (v0 * a.ys) * a.dt, 0.0f, ymax);
-        const float pzp = clampf(z0 + (w0 * a.zs) * a.dt, 0.0f, ztop);
-        const float3 s1 = sample_dual(a, s_heights, pxp, pyp, pzp);
-        const float u1 = s1.x + tu, v1 = s1.y + tv, w1 = s1.z;
-        const float cu = 0.5f * (u0 + u1), cv = 0.5f * (v0 + v1), cw = 0.5f * (w0 + w1);
-        const float x1 = clampf(x0 + (cu * a.xs) * a.dt, 0.0f, xmax);
-        const float y1 = clampf(y0 + (cv * a.ys) * a.dt, 0.0f, ymax);
-        pz = clampf(z0 + (cw * a.zs) * a.dt, 0.0f, ztop);
-        split_coord(x1, a.nx, cx, px);
-        split_coord(y1, a.ny, cy, py);
-        a.cell_x[p] = cx; a.cell_y[p] = cy;
-        a.pos_x[p] = px; a.pos_y[p] = py;
-        a.vel_u[p] = cu; a.vel_v[p] = cv; a.vel_w[p] = cw;
-    }
-
-    // ---- langevin_fused.wgsl:414-515 ----
-    if (turb_on) {
-        const float x = (float)cx + px;
-        const float y = (float)cy + py;
-        const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(a.pnx - 1u)));
-        const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(a.pny - 1u)));
-        const float4 cell = __ldg(a.pbl + (i * a.pny + j));
-        const Hanna hn = compute_hanna(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
-
-        const uint32_t n_vert = a.n_sub > 1u ? a.n_sub : 1u;
-        const uint32_t blocks = (2u + n_vert + 3u) / 4u;
-        const u32x4 b0 = philox4x32_10(counter_add(a.counter, p * blocks), a.key0, a.key1);
-        u32x4 b1 = {0u, 0u, 0u, 0u};
-        if (blocks > 1u) b1 = philox4x32_10(counter_add(a.counter, p * blocks + 1u), a.key0, a.key1);
-        const float2 e_uv = box_muller(u32_to_uniform01(b0.x), u32_to_uniform01(b0.y));
-        const float2 e_w01 = box_muller(u32_to_uniform01(b0.z), u32_to_uniform01(b0.w));
-        const float2 e_w23 = box_muller(u32_to_uniform01(b1.x), u32_to_uniform01(b1.y));
-
-        tu = langevin_h(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
-        tv = langevin_h(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
-        float tw = a.turb_w[p];
-        if (a.n_sub == 0u) {
-            tw = langevin_v(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
-        } else {
-            int32_t cbt = a.cbt[p];
-            const int32_t cbt_in = cbt;
-            const float dt_sub = a.tdt / (float)a.n_sub;
-            const float h = hn.h;
-            const float zmin = a.zmin;
-            float sigw = hn.sigw, dsigwdz = hn.dsigwdz, tlw = hn.tlw;
-            for (uint32_t sub = 0; sub < a.n_sub; ++sub) {
-                const float eta = sub == 0u ? e_w01.x : sub == 1u ? e_w01.y : sub == 2u ? e_w23.x : e_w23.y;
-                tw = langevin_v(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
-                pz = pz + tw * dt_sub;
-                if (h > zmin) {
-                    float z = pz;
-                    for (int bounce = 0; bounce < 10; ++bounce) {
-                        if (z < zmin) { z = 2.0f * zmin - z; cbt = -cbt; tw = -tw; }
-                        else if (z > h) { z = 2.0f * h - z; cbt = -cbt; tw = -tw; }
-                        else break;
-                    }
-                    pz = clampf(z, zmin, h);
-                }
-                if (sub < a.n_sub - 1u) hanna_short_w(hn.ust, hn.wst, hn.ol, hn.h, pz, sigw, dsigwdz, tlw);
-            }
-            if (cbt != cbt_in) a.cbt[p] = cbt;
-        }
-        a.turb_u[p] = tu; a.turb_v[p] = tv; a.turb_w[p] = tw;
-    }
-    if ((a.stages & FPG_STAGE_ADVECT) || (turb_on && a.n_sub != 0u)) a.pos_z[p] = pz;
-
-    // ---- dry_deposition.wgsl:89-105 and wet_deposition.wgsl:203-216 ----
-    if (dry_on || wet_on) {
-        float survival = 1.0f;
-        if (dry_on) {
-            float prob = 0.0f;
-            if (!(pz >= 2.0f * a.href)) {
-                const float vd = a.dry_mode == FPG_FORCING_PER_PARTICLE ? a.dry_v_arr[p] : a.dry_v;
-                const float s = dry_survival(vd, a.tdt, a.href);
-                prob = 1.0f - s;
-                survival = s;
-            }
-            if (a.dry_prob) a.dry_prob[p] = prob;
-        }
-        float wsurv = 1.0f;
-        if (wet_on) {
-            float lam, fr;
-            if (a.wet_mode == FPG_FORCING_PER_PARTICLE) {
-                lam = a.wet_l_arr[p]; fr = a.wet_f_arr[p];
-            } else if (a.wet_mode == FPG_FORCING_PER_CELL) {
-                const float x = (float)cx + px;
-                const float y = (float)cy + py;
-                const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(a.wnx - 1u)));
-                const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(a.wny - 1u)));
-                const float2 c = __ldg(a.wet_cells + (i * a.wny + j));
-                lam = c.x; fr = c.y;
-            } else {
-                lam = a.wet_l; fr = a.wet_f;
-            }
-            const float prob = wet_probability(lam, a.tdt, fr);
-            wsurv = 1.0f - prob;
-            if (a.wet_prob) a.wet_prob[p] = prob;
-        }
-        // mass * dry survival, then * wet survival: two roundings, as the
-        // two reference passes apply them.
-        for (int k = 0; k < a.n_species; ++k) {
-            float m = a.mass[k][p];
-            if (dry_on && !(pz >= 2.0f * a.href)) m = m * survival;
-            if (wet_on) m = m * wsurv;
-            a.mass[k][p] = m;
-        }
-    }
+    particle_step(a, s_heights, p, p, a.alpha, a.counter, a.key0, a.key1);
 }
 
 // ---- per-cell kernels --------------------------------------------------------
 
-__device__ __forceinline__ float sp_(float v, float fb) { return (finitef(v) && v > 0.0f) ? v : fb; }
-__device__ __forceinline__ float snn_(float v, float fb) { return (finitef(v) && v >= 0.0f) ? v : fb; }
-__device__ __forceinline__ float sf_(float v, float fb) { return finitef(v) ? v : fb; }
-
-// interpolate_surface_fields_linear (io/temporal.rs:99-104,122-214) followed
-// by pbl_diagnostics.wgsl:238-305 for one cell.
 __global__ void __launch_bounds__(256) pbl_diag_kernel(const fpg_surface_cell* __restrict__ s0,
                                                        const fpg_surface_cell* __restrict__ s1, float alpha,
                                                        fpg_pbl_options o, uint32_t ncell, float* ustar_o,
@@ -321,77 +54,7 @@ __global__ void __launch_bounds__(256) pbl_diag_kernel(const fpg_surface_cell* _
                                                        float* ssr_o, float* surfstr_o, float4* packed) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
-    float in[10];
-    const float* a = &s0[c].surface_pressure_pa;
-    const float* b = &s1[c].surface_pressure_pa;
-#pragma unroll
-    for (int k = 0; k < 10; ++k) {
-        if (alpha <= 0.0f) in[k] = a[k];
-        else if (alpha >= 1.0f) in[k] = b[k];
-        else in[k] = lerpf(a[k], b[k], alpha);
-    }
-    const float sp = in[0], t2 = in[1], u10 = in[2], v10 = in[3], stress = in[4], shf = in[5], ssr = in[6];
-    const float hm = in[7], fv = in[8], oli_in = in[9];
-    const float temp_k = sp_(t2, 300.0f);
-    const float pressure = sp_(sp, 101325.0f);
-    const float air_density = pressure / (287.05f * temp_k);
-    float est;
-    {
-        const float rho = sp_(air_density, 1.225f);
-        const float safe_stress = snn_(stress, 0.0f);
-        if (safe_stress > 0.0f) {
-            est = fmaxf(sqrtf(safe_stress / rho), 1.0e-4f);
-        } else {
-            const float z0 = sp_(o.roughness_length_m, 0.1f);
-            const float zr = fmaxf(sp_(o.wind_reference_height_m, 10.0f), 1.01f * z0);
-            const float ws = fmaxf(sqrtf(u10 * u10 + v10 * v10), 0.0f);
-            if (ws <= 0.0f) {
-                est = 1.0e-4f;
-            } else {
-                const float us = 0.4f * ws / fmaxf(logf(zr / z0), 1.0e-6f);
-                est = fmaxf(sp_(us, 1.0e-4f), 1.0e-4f);
-            }
-        }
-    }
-    const float ustar = (finitef(fv) && fv > 0.0f) ? fmaxf(fv, 1.0e-4f) : fmaxf(est, 1.0e-4f);
-    float computed_ol;
-    {
-        const float hf = sf_(shf, 0.0f);
-        if (fabsf(hf) < fmaxf(o.heat_flux_neutral_threshold_w_m2, 0.0f)) {
-            computed_ol = __int_as_float(0x7f800000);
-        } else {
-            const float u = fmaxf(sp_(ustar, 1.0e-4f), 1.0e-4f);
-            const float t = sp_(temp_k, 300.0f);
-            const float d = sp_(air_density, 1.225f);
-            const float numerator = -(d * 1004.6f * t * u * u * u);
-            const float denominator = 0.4f * 9.81f * hf;
-            if (fabsf(denominator) < 1.0e-9f) {
-                computed_ol = __int_as_float(0x7f800000);
-            } else {
-                const float olv = numerator / denominator;
-                computed_ol = (!finitef(olv) || fabsf(olv) > 1.0e9f) ? __int_as_float(0x7f800000) : olv;
-            }
-        }
-    }
-    float oli;
-    if (finitef(oli_in) && fabsf(oli_in) >= 1.0e-5f) oli = oli_in;
-    else oli = (!finitef(computed_ol) || fabsf(computed_ol) > 1.0e5f) ? 0.0f : 1.0f / computed_ol;
-    const float hsrc = (finitef(hm) && hm > 0.0f) ? hm : o.fallback_mixing_height_m;
-    const float hmix = fmaxf(clampf(hsrc, o.hmix_min_m, o.hmix_max_m), o.hmix_min_m);
-    const float safe_shf = sf_(shf, 0.0f);
-    float wstar = 0.0f;
-    if (safe_shf > 0.0f) {
-        const float d = sp_(air_density, 1.225f);
-        const float t = sp_(temp_k, 300.0f);
-        const float hh = sp_(hmix, o.hmix_min_m);
-        const float bf = safe_shf / (d * 1004.6f) * 9.81f / t;
-        if (!(bf <= 0.0f || !finitef(bf))) wstar = fmaxf(powf(bf * hh, 1.0f / 3.0f), 0.0f);
-    }
-    ustar_o[c] = ustar; wstar_o[c] = wstar; hmix_o[c] = hmix; oli_o[c] = oli;
-    sshf_o[c] = sf_(shf, 0.0f);
-    ssr_o[c] = snn_(ssr, 0.0f);
-    surfstr_o[c] = snn_(stress, 0.0f);
-    packed[c] = make_float4(ustar, wstar, hmix, oli);
+    pbl_cell(s0, s1, alpha, o, c, ustar_o, wstar_o, hmix_o, oli_o, sshf_o, ssr_o, surfstr_o, packed);
 }
 
 __global__ void __launch_bounds__(256) pack_pbl_kernel(const float* __restrict__ u, const float* __restrict__ w,
@@ -408,11 +71,6 @@ __global__ void __launch_bounds__(256) pack_frame_kernel(const float* __restrict
     if (n < nodes) bracket[2u * n + (uint32_t)which] = make_float4(u[n], v[n], w[n], 0.0f);
 }
 
-__device__ __forceinline__ float snn0(float v) { return (finitef(v) && v > 0.0f) ? v : 0.0f; }
-__device__ __forceinline__ int precip_class(float p) {
-    return p > 20.0f ? 4 : p > 8.0f ? 3 : p > 3.0f ? 2 : p > 1.0f ? 1 : 0;
-}
-
 // wet_precipitation_state + below_cloud_scavenging_coefficient_gas
 // (physics/wet_scavenging.rs:179-225,78-82) per met cell.
 __global__ void __launch_bounds__(256) wet_cells_kernel(const float* __restrict__ lsp_in,
@@ -421,25 +79,7 @@ __global__ void __launch_bounds__(256) wet_cells_kernel(const float* __restrict_
                                                         uint32_t ncell, float2* out) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
-    const float lsf[5] = {0.5f, 0.65f, 0.8f, 0.9f, 0.95f};
-    const float cvf[5] = {0.4f, 0.55f, 0.7f, 0.8f, 0.9f};
-    const float lsp = snn0(lsp_in[c]), convp = snn0(conv_in[c]);
-    const float total = lsp + convp;
-    float fraction = 0.0f, subgrid = 0.0f;
-    if (!(total < 0.01f)) {
-        const float cc = clampf(cc_in[c], 0.0f, 1.0f);
-        const float weighted = (lsp * lsf[precip_class(lsp)] + convp * cvf[precip_class(convp)]) / fmaxf(total, 1.0e-12f);
-        const float area = fminf(fmaxf(fmaxf(cc * weighted, 0.05f), 0.05f), 1.0f);
-        subgrid = snn0(total / fmaxf(area, 1.0e-12f));
-        fraction = area;
-    }
-    float lambda = 0.0f;
-    if (total >= 0.01f && fraction > 0.0f && subgrid > 0.0f) {
-        lambda = snn0(snn0(a_in) * powf(subgrid, snn0(b_in)));
-    } else {
-        fraction = 0.0f;
-    }
-    out[c] = make_float2(lambda, fraction);
+    out[c] = wet_cell_forcing(lsp_in[c], conv_in[c], cc_in[c], a_in, b_in);
 }
 
 __global__ void __launch_bounds__(256) fill_kernel(float* out, uint32_t n, float v) {

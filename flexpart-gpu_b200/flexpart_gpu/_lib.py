@@ -116,6 +116,20 @@ _sig("fpg_forward_run_timestep", _i32, _vp, _vp, _vp, _vp)
 _sig("fpg_forward_finalize", _i32, _vp)
 _sig("fpg_forward_particles", _vp, _vp)
 _sig("fpg_forward_accumulate_grid", _i32, _vp, _vp, _u32, _f32, _vp, _sz)
+_sig("fpg_batch_create", _i32, _vp, _vp, _vp, _sz, _sz, _sz, _sz, _vp, ctypes.POINTER(_vp))
+_sig("fpg_batch_destroy", _i32, _vp)
+_sig("fpg_batch_upload_frame", _i32, _vp, _u32, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_batch_run", _i32, _vp, _u32, _i32)
+_sig("fpg_batch_run_sequential", _i32, _vp, _u32)
+_sig("fpg_batch_steps_done", ctypes.c_uint64, _vp)
+_sig("fpg_batch_scenario_slots", _i32, _vp, _sz, ctypes.POINTER(_sz), ctypes.POINTER(_sz))
+_sig("fpg_batch_particles", _vp, _vp)
+_sig("fpg_batch_download_grids", _i32, _vp, _vp, _vp)
+_sig("fpg_batch_errors", _i32, _vp, ctypes.POINTER(_i32))
+_sig("fpg_batch_tuning_candidates", _u32, _vp, _u32)
+_sig("fpg_batch_autotune", _i32, _vp, _u32, _vp, _u32, _vp)
+_sig("fpg_batch_set_tuning", _i32, _vp, _vp)
+_sig("fpg_batch_get_tuning", _i32, _vp, _vp)
 _sig("fpg_sorter_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
 _sig("fpg_sorter_destroy", _i32, _vp)
 _sig("fpg_sort_by_cell", _i32, _vp, _vp, _vp, _vp, _vp, _vp)
@@ -154,4 +168,8 @@ EXPORTED_DRIVER = [
     "fpg_forward_config_default", "fpg_forward_create", "fpg_forward_destroy", "fpg_forward_has_remaining_steps",
     "fpg_forward_current_time", "fpg_forward_run_timestep", "fpg_forward_finalize", "fpg_forward_particles",
     "fpg_forward_accumulate_grid", "fpg_parse_timestamp",
+    "fpg_batch_create", "fpg_batch_destroy", "fpg_batch_upload_frame", "fpg_batch_run", "fpg_batch_run_sequential",
+    "fpg_batch_steps_done", "fpg_batch_scenario_slots", "fpg_batch_particles", "fpg_batch_download_grids",
+    "fpg_batch_errors", "fpg_batch_tuning_candidates", "fpg_batch_autotune", "fpg_batch_set_tuning",
+    "fpg_batch_get_tuning",
 ]

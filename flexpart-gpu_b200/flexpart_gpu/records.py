@@ -171,6 +171,42 @@ class ForwardConfig(ctypes.Structure):
     ]
 
 
+class BatchScenario(ctypes.Structure):
+    """``fpg_batch_scenario``: one release with its own Philox key and
+    initial counter (include/fpg_driver.h)."""
+
+    _fields_ = [("release", Release), ("key", ctypes.c_uint32 * 2), ("counter", ctypes.c_uint32 * 4)]
+
+
+class BatchConfig(ctypes.Structure):
+    """``fpg_batch_config``: the shared clock, met ring, physics options and
+    per-scenario output grid of a batched ensemble."""
+
+    _fields_ = [
+        ("start_seconds", ctypes.c_int64), ("end_seconds", ctypes.c_int64), ("timestep_seconds", ctypes.c_int64),
+        ("frame_seconds", ctypes.c_int64), ("n_frames", ctypes.c_uint32),
+        ("x_grid_per_meter", ctypes.c_float), ("y_grid_per_meter", ctypes.c_float),
+        ("z_grid_per_meter", ctypes.c_float),
+        ("pbl_options", PblOptions),
+        ("dry_reference_height_m", ctypes.c_float), ("dry_velocity_m_s", ctypes.c_float),
+        ("rho_grad_over_rho", ctypes.c_float), ("n_substeps", ctypes.c_uint32), ("min_height_m", ctypes.c_float),
+        ("wet_from_precipitation", ctypes.c_int32), ("wet_gas_a", ctypes.c_float), ("wet_gas_b", ctypes.c_float),
+        ("release_grid", GridDomain),
+        ("out_nx", ctypes.c_uint32), ("out_ny", ctypes.c_uint32), ("out_nz", ctypes.c_uint32),
+        ("outheights", ctypes.c_void_p), ("output_every_steps", ctypes.c_uint32),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    """``fpg_batch_tuning``: launch shape of the batched particle pass."""
+
+    _fields_ = [("block_threads", ctypes.c_uint32), ("min_blocks_per_sm", ctypes.c_uint32),
+                ("particles_per_thread", ctypes.c_uint32), ("step_ms", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class MetBracket(ctypes.Structure):
     """``fpg_met_bracket``: MetTimeBracket (timeloop.rs:270-285)."""
 

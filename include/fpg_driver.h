@@ -131,6 +131,107 @@ fpg_particles* fpg_forward_particles(fpg_forward* d);
 fpg_status fpg_forward_accumulate_grid(fpg_forward* d, fpg_grid* grid, uint32_t species_index,
                                        float mass_scale, const float* outheights, size_t n_outheights);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble: many independent release scenarios stepped together.
+ *
+ * No counterpart in the reference, which runs one scenario per driver.  Each
+ * scenario is what one ForwardTimeLoopDriver with one release, capacity =
+ * its particle_count, its own Philox key and initial counter would compute
+ * (the same release lattice, slots, counters and kernels), so its particles
+ * come out bit for bit as in a plain run of it alone.  All scenarios share
+ * one met frame ring and one global clock; their particles sit in one
+ * structure-of-arrays population, each scenario in a 256-slot-aligned
+ * segment.  One step is a CUDA graph of device-side kernels (clock and
+ * release bookkeeping, bracket repack when it changes, per-cell PBL and wet
+ * forcing, release of new particles, one persistent launch over all
+ * scenarios' tiles from a work queue, per-scenario grids at output steps,
+ * counter advance), so the host only launches the graph.
+ * ---------------------------------------------------------------------- */
+typedef struct fpg_batch_scenario {
+    fpg_release release;
+    uint32_t key[2];
+    uint32_t counter[4];
+} fpg_batch_scenario;
+
+typedef struct fpg_batch_config {
+    int64_t start_seconds, end_seconds, timestep_seconds;
+    int64_t frame_seconds;          /* frames k at start + k*frame_seconds, cycled */
+    uint32_t n_frames;
+    float x_grid_per_meter, y_grid_per_meter, z_grid_per_meter;
+    fpg_pbl_options pbl_options;
+    float dry_reference_height_m;
+    float dry_velocity_m_s;         /* 0: no dry deposition */
+    float rho_grad_over_rho;
+    uint32_t n_substeps;
+    float min_height_m;
+    int32_t wet_from_precipitation; /* per-cell wet forcing from each bracket's t0 precipitation */
+    float wet_gas_a, wet_gas_b;
+    fpg_grid_domain release_grid;
+    uint32_t out_nx, out_ny, out_nz;
+    const float* outheights;        /* out_nz heights (copied at create) */
+    uint32_t output_every_steps;    /* grids at steps k with (k+1) % every == 0; 0: never */
+} fpg_batch_config;
+
+typedef struct fpg_batch fpg_batch;
+
+/* 1 <= n_scenarios <= 65535; every particle_count and release window below
+ * 2^32 (FPG_ERR_VALUE_TOO_LARGE); FPG_ERR_OUT_OF_GRID when a scenario's
+ * release lattice leaves release_grid, as the release manager reports it at
+ * injection (release/mod.rs:41). */
+fpg_status fpg_batch_create(fpg_ctx* ctx, const fpg_batch_config* cfg, const fpg_batch_scenario* scenarios,
+                            size_t n_scenarios, size_t met_nx, size_t met_ny, size_t met_nz,
+                            const float* level_heights, fpg_batch** out);
+fpg_status fpg_batch_destroy(fpg_batch* b);
+/* Frame k of the met ring: u, v, w (nx*ny*nz, reference layout), surface
+ * cells (nx*ny) and large-scale precipitation [mm/h] (nx*ny, may be NULL). */
+fpg_status fpg_batch_upload_frame(fpg_batch* b, uint32_t k, const float* u, const float* v, const float* w,
+                                  const fpg_surface_cell* surface, const float* precipitation_mm_h);
+/* Runs n_steps steps (fewer if the end time comes first): each step is one
+ * replay of the captured graph when use_graph is non-zero (the graph is
+ * captured on the first call), else the same kernels launched one by one.
+ * Returns FPG_ERR_SIMULATION_COMPLETE when no step is left. */
+fpg_status fpg_batch_run(fpg_batch* b, uint32_t n_steps, int32_t use_graph);
+/* The same steps with one plain fused-step launch per scenario per step
+ * (sequential launches, no graph): the comparison the batching is measured
+ * against.  Bit-identical results. */
+fpg_status fpg_batch_run_sequential(fpg_batch* b, uint32_t n_steps);
+/* Steps taken so far; slot range of scenario s; the whole population. */
+uint64_t fpg_batch_steps_done(const fpg_batch* b);
+fpg_status fpg_batch_scenario_slots(const fpg_batch* b, size_t s, size_t* first_slot, size_t* count);
+fpg_particles* fpg_batch_particles(fpg_batch* b);
+/* Per-scenario grids of the last output step: n_scenarios * out cells each
+ * (scenario-major), u32 counts and scaled masses (scale 1e6). */
+fpg_status fpg_batch_download_grids(fpg_batch* b, uint32_t* counts, uint32_t* mass_scaled);
+/* Device-side error flags (1: a release fell outside the grid). */
+fpg_status fpg_batch_errors(fpg_batch* b, int32_t* flags);
+
+/* Launch shape of the persistent particle pass: threads per CTA, CTAs
+ * resident per SM the kernel is compiled for (its register budget), and
+ * particles per thread in one work item (a work item is block_threads *
+ * particles_per_thread consecutive slots of one scenario).  step_ms is the
+ * particle pass's time measured by the tuner (0 when set by hand). */
+typedef struct fpg_batch_tuning {
+    uint32_t block_threads;
+    uint32_t min_blocks_per_sm;
+    uint32_t particles_per_thread;
+    float step_ms;
+} fpg_batch_tuning;
+
+/* The compiled launch shapes: writes up to max of them, returns their count. */
+uint32_t fpg_batch_tuning_candidates(fpg_batch_tuning* out, uint32_t max);
+/* Times the next step's particle pass under every compiled shape (best of
+ * reps), each from the same snapshot of the live state, restores the state
+ * and keeps the fastest shape.  Results are identical under every shape.
+ * Needs device memory for one copy of the population.  results (up to
+ * max_results entries, candidate order) and best may be NULL.  Call it once
+ * the population is representative (after some steps), or tune a copy of the
+ * run and pass the choice to fpg_batch_set_tuning. */
+fpg_status fpg_batch_autotune(fpg_batch* b, uint32_t reps, fpg_batch_tuning* results, uint32_t max_results,
+                              fpg_batch_tuning* best);
+/* Selects a compiled shape (FPG_ERR_INVALID_ARGUMENT if none matches). */
+fpg_status fpg_batch_set_tuning(fpg_batch* b, const fpg_batch_tuning* tuning);
+fpg_status fpg_batch_get_tuning(const fpg_batch* b, fpg_batch_tuning* tuning);
+
 /* parse_timestamp_seconds (release/mod.rs:283-334): "YYYYMMDDHHMMSS". */
 fpg_status fpg_parse_timestamp(const char* yyyymmddhhmmss, int64_t* seconds);
 

@@ -40,3 +40,51 @@ def test_null_handles_are_rejected():
     assert lib.fpg_step(None, None, None, None, None, None, None) == -1
     assert lib.fpg_particles_upload(None, 0, 0, None, None) == -1
     assert lib.fpg_grid_download(None, None, None, None, None) == -1
+
+
+def test_record_layouts_match_the_c_header(tmp_path):
+    """Every ctypes record the host side passes through the ABI has the size
+    and field offsets the C compiler gives the header's struct."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from flexpart_gpu import records as R
+
+    gcc = shutil.which("gcc") or "/usr/bin/gcc"
+    pairs = {
+        "fpg_step_params": R.StepParams, "fpg_pbl_options": R.PblOptions, "fpg_release": R.Release,
+        "fpg_grid_domain": R.GridDomain, "fpg_forward_config": R.ForwardConfig, "fpg_met_bracket": R.MetBracket,
+        "fpg_forcing": R.Forcing, "fpg_step_report": R.StepReport, "fpg_batch_scenario": R.BatchScenario,
+        "fpg_batch_tuning": R.BatchTuning,
+        "fpg_batch_config": R.BatchConfig,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fpg_driver.h"', "int main(void) {"]
+    for c, py in pairs.items():
+        lines.append(f'printf("{c} size %zu\\n", sizeof({c}));')
+        for name, _ in py._fields_:
+            lines.append(f'printf("{c} {name} %zu\\n", offsetof({c}, {name}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(ROOT, "include")
+    subprocess.run([gcc, "-I", str(inc), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        c, name, v = line.split()
+        got[(c, name)] = int(v)
+    for c, py in pairs.items():
+        assert got[(c, "size")] == ctypes.sizeof(py), c
+        for name, _ in py._fields_:
+            assert got[(c, name)] == getattr(py, name).offset, (c, name)
+
+
+def test_batch_tuning_candidates_listed_without_a_device():
+    from flexpart_gpu.batch import tuning_candidates
+
+    c = tuning_candidates()
+    assert len(c) >= 4
+    shapes = {(t["block_threads"], t["min_blocks_per_sm"], t["particles_per_thread"]) for t in c}
+    assert (256, 4, 1) in shapes
+    assert len(shapes) == len(c)
