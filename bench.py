@@ -22,6 +22,10 @@ concentration grid is read back every step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+The line's "batched" object is the batched ensemble (run_batched): 256
+release scenarios stepped as one population, one CUDA-graph replay per step,
+against interleaved plain launches and scenario-by-scenario driver runs.
+
 Under torchrun each rank runs its own 10 M-particle shard (weak scaling, met
 replicated, no exchange in the timed region).  Rank 0 prints one JSON line.
 """
@@ -63,6 +67,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-scenarios", type=int, default=256)
     ap.add_argument("--quick", action="store_true",
                     help="profiling case: no spin-up (particles scattered around the sources), no e2e, no CPU leg")
     return ap.parse_args()
@@ -210,6 +216,152 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_batched(ctx, stream, args, rank, world):
+    """The batched ensemble: 256 release scenarios (particle counts
+    log-uniform in [10 k, 1 M], about 54 M in all, own source, start time and
+    Philox key) on met 180x90x40 with 9 frames, 24 h at dt 900 s (97 steps),
+    per-scenario output grids 180x90x3 every 3 h.  One full 24 h run is timed
+    (device events, max over ranks) after a tuning pass of the launch shape;
+    beside it the same run as interleaved plain launches (one fused-step
+    launch per scenario per step) and as scenario-by-scenario plain driver
+    runs (a subset, scaled by particle-steps)."""
+    import torch
+    import torch.distributed as dist
+
+    from flexpart_gpu import api, synthetic
+    from flexpart_gpu import batch as bt
+    from flexpart_gpu import timeloop as tl
+
+    ens = synthetic.config2(n_scenarios=args.batch_scenarios, seed=2 + rank)
+    spec = ens.met
+    n = ens.n_steps
+    ps = bt.particle_steps(ens)
+    heights = synthetic.level_heights(spec.nz, spec.top_m)
+    frames = synthetic.make_frames(spec)
+    precs = [synthetic.precipitation(spec, k) for k in range(spec.n_frames)]
+
+    def make():
+        b = bt.Batch(ctx, bt.ensemble_config(ens, output_every_steps=12), bt.ensemble_scenarios(ens),
+                     (spec.nx, spec.ny, spec.nz), heights, ens.outheights)
+        for k, f in enumerate(frames):
+            b.upload_frame(k, f, precs[k])
+        return b
+
+    def timed(fn):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        ctx.synchronize()
+        ms = a.elapsed_time(b)
+        if world > 1:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms
+
+    # launch shape chosen on a copy of the run at 3/4 of its length
+    b = make()
+    k_tune = 3 * n // 4
+    b.run(k_tune)
+    best, cands = b.autotune(reps=3)
+    pass_particles = bt.particle_steps(ens, k_tune, 1)
+    del b
+    # warm-up run, then the timed run
+    b = make()
+    b.tuning = best
+    b.run(n)
+    del b
+    b = make()
+    b.tuning = best
+    l0 = ctx.kernel_launches
+    ms = timed(lambda: b.run(n))
+    launches = ctx.kernel_launches - l0
+    errors = b.errors()
+    del b
+    b = make()
+    ms_seq = timed(lambda: b.run_sequential(n))
+    del b
+
+    # end to end through the public calls: met ring from host, run, grids back
+    counts_h = np.empty((len(ens.sources),) + tuple(ens.out_shape), np.uint32)
+    h2d = 0
+    for f, p in zip(frames, precs):
+        h2d += 3 * f["u"].nbytes + f["surface"].nbytes + p.nbytes
+    b = make()
+    b.tuning = best
+
+    def e2e():
+        for k, f in enumerate(frames):
+            b.upload_frame(k, f, precs[k])
+        b.run(n)
+        c, m = b.download_grids()
+        counts_h[...] = c
+
+    ms_e2e = timed(e2e)
+    del b
+
+    # scenario-by-scenario plain driver runs over a subset
+    sub = min(16, len(ens.sources))
+    ps_sub = 0
+    t_drv = 0.0
+    for s in range(sub):
+        scn = ens.scenario(s)
+        drv = tl.ForwardDriver(ctx, tl.scenario_config(scn), tl.scenario_releases(scn), tl.scenario_domain(scn),
+                               scn.capacity, (spec.nx, spec.ny, spec.nz), heights)
+        src = tl.BracketSource(scn, frames)
+        cells = api.CellField(ctx, spec.nx, spec.ny)
+        forcing = tl.cell_forcing(cells, dry_velocity=ens.dry_velocity)
+
+        def run_one():
+            last = None
+            for _ in range(n):
+                t = drv.current_time_seconds
+                fa = synthetic.bracket_frames(scn, t)[0]
+                if fa != last:
+                    cells.from_precipitation(precs[fa], a=ens.wet_a, b=ens.wet_b)
+                    last = fa
+                drv.run_timestep(src.at(t), forcing)
+
+        t_drv += timed(run_one) / 1e3
+        one = synthetic.Ensemble(ens.name, spec, [ens.sources[s]], [ens.keys[s]], ens.start, ens.end, ens.dt,
+                                 ens.out_shape, ens.outheights)
+        ps_sub += bt.particle_steps(one)
+        del drv, cells
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = BYTES_PER_PARTICLE_STEP * pass_particles / (best["step_ms"] / 1e3) / 1e9
+    value = ps * world / (ms / 1e3)
+    return {
+        "workload": f"{len(ens.sources)} release scenarios, {ens.total_particles} particles (log-uniform "
+                    f"[10k, 1M] per scenario), met {spec.nx}x{spec.ny}x{spec.nz}, 9 frames, 24 h, {n} steps, "
+                    f"per-scenario grids {ens.out_shape[0]}x{ens.out_shape[1]}x{ens.out_shape[2]} every 3 h",
+        "value": value, "unit": UNIT, "particle_steps_per_run": ps, "ms_per_run": ms,
+        "gpu_launches": int(launches), "errors": errors,
+        "tuning": best, "tuning_candidates": cands,
+        "sequential_interleaved": {"value": ps * world / (ms_seq / 1e3), "ms_per_run": ms_seq,
+                                   "path": "fpg_batch_run_sequential: one fused_step_kernel launch per scenario "
+                                           "per step, shared per-step kernels, no graph"},
+        "per_scenario_driver": {"value": ps_sub / t_drv, "scenarios_timed": sub, "seconds": t_drv,
+                                "path": "fpg_forward_run_timestep per scenario, one plain run after another, "
+                                        "met from host"},
+        "speedup_vs_interleaved": ms_seq / ms,
+        "speedup_vs_per_scenario_driver": value / world / (ps_sub / t_drv),
+        "e2e": {"value": ps * world / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_run": h2d,
+                "d2h_bytes_per_run": 2 * counts_h.nbytes,
+                "path": "fpg_batch_upload_frame x9 + fpg_batch_run + fpg_batch_download_grids"},
+        "roofline": {"bound": "hbm", "kernel": "batch_step_kernel", "particles_per_launch": pass_particles,
+                     "kernel_ms": best["step_ms"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind},
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -415,6 +567,10 @@ def main():
                "sample": f"the first {sample} particles of the spun-up population x {len(times)} production steps "
                          f"(oracle C restatement, {threads} OpenMP threads, {sum(times):.1f} s)"}
 
+    batched = None
+    if not args.no_batched and not args.quick:
+        batched = run_batched(ctx, stream, args, rank, world)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -436,6 +592,7 @@ def main():
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     del drv
