@@ -29,10 +29,9 @@
 #include <vector>
 
 #include "../../include/fpg_driver.h"
+#include "batch_core.cuh"
 #include "fpg_internal.h"
 #include "grid_core.cuh"
-#include "physics.cuh"
-#include "step_core.cuh"
 
 namespace fpg {
 
@@ -43,52 +42,6 @@ __global__ void __launch_bounds__(256, 4) fused_step_kernel(StepArgs a);
 
 namespace {
 
-constexpr uint32_t TILE = 256;
-
-struct BatchState {
-    int64_t t;
-    int64_t ta;
-    uint32_t step;
-    int32_t fa, fb;
-    int32_t have_bracket;
-    int32_t changed;
-    float alpha;
-    int32_t error;
-    uint32_t work;
-};
-
-struct ScenDev {
-    uint32_t offset, capacity, first_tile, n_tiles;
-    uint32_t key0, key1;
-    u32x4 counter;
-    uint32_t released, rel_lo, rel_hi;
-    float mass_per_particle;
-    int64_t start, end;
-    double lon_min, lon_max, lat_min, lat_max, z_min, z_max;
-    uint64_t count;
-    uint64_t lat_nx, lat_nxy, lat_nz;
-};
-
-struct BatchConst {
-    int64_t start, frame_seconds, dt;
-    uint32_t n_frames;
-    uint32_t n_scen;
-    uint32_t n_tiles;
-    uint32_t bpp;
-    double xlon0, ylat0, dx, dy;
-    uint64_t gnx, gny;
-};
-
-// ReleaseState::target_emitted_count (release/mod.rs:181-196); counts and
-// window lengths are below 2^32 (checked at create), so the u128 product of
-// the reference fits in 64 bits.
-__host__ __device__ inline uint32_t target_emitted(int64_t start, int64_t end, uint64_t count, int64_t now,
-                                                   uint32_t released) {
-    if (now < start || now > end) return released;
-    if (start == end) return (uint32_t)count;
-    if (now == end) return (uint32_t)count;
-    return (uint32_t)((count * (uint64_t)(now - start)) / (uint64_t)(end - start));
-}
 
 __global__ void batch_advance_kernel(BatchState* st, ScenDev* sc, BatchConst c) {
     const int64_t t = st->t;
@@ -140,8 +93,6 @@ __global__ void __launch_bounds__(256) batch_pbl_kernel(const BatchState* st, co
              f6, packed);
     if (wet_on && st->changed) wet[c] = wet_cell_forcing(precip[(size_t)st->fa * ncell + c], 0.0f, 1.0f, wa, wb);
 }
-
-struct PopFields { uint32_t* f[FPG_FIELD_COUNT]; };
 
 // ReleaseManager::inject_for_time + geo_to_grid + to_relative
 // (release/mod.rs:103-146, coords/mod.rs:92-114,169-178) on the device, in
@@ -222,7 +173,7 @@ const StepVariant kVariants[] = {
     {128, 8, 1, batch_step_kernel<128, 8, 1>}, {128, 8, 2, batch_step_kernel<128, 8, 2>},
     {512, 2, 1, batch_step_kernel<512, 2, 1>},
 };
-constexpr uint32_t kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+static_assert(sizeof(kVariants) / sizeof(kVariants[0]) == kNumVariants, "launch shape table");
 
 struct GridConst {
     uint32_t nx, ny, nz, cells;
@@ -280,22 +231,6 @@ __global__ void __launch_bounds__(256) batch_grid_kernel(const BatchState* st, c
     }
 }
 
-__host__ __device__ inline u32x4 counter_add64(u32x4 c, uint64_t off) {
-    // philox_counter_add (rng.rs:69-87)
-    const uint32_t lo = (uint32_t)off, hi = (uint32_t)(off >> 32);
-    u32x4 r;
-    r.x = c.x + lo;
-    const uint32_t carry0 = r.x < c.x;
-    const uint32_t n1 = c.y + hi;
-    const uint32_t carry1a = n1 < c.y;
-    r.y = n1 + carry0;
-    const uint32_t carry1b = r.y < n1;
-    r.z = c.z + (carry1a | carry1b);
-    const uint32_t carry2 = r.z < c.z;
-    r.w = c.w + carry2;
-    return r;
-}
-
 __global__ void batch_end_kernel(BatchState* st, ScenDev* sc, BatchConst c) {
     for (uint32_t s = threadIdx.x; s < c.n_scen; s += blockDim.x)
         sc[s].counter = counter_add64(sc[s].counter, (uint64_t)sc[s].capacity * c.bpp);
@@ -306,46 +241,8 @@ __global__ void batch_end_kernel(BatchState* st, ScenDev* sc, BatchConst c) {
 }
 
 }  // namespace
-}  // namespace fpg
 
-using namespace fpg;
-
-struct fpg_batch {
-    fpg_ctx* ctx = nullptr;
-    fpg_batch_config cfg{};
-    std::vector<float> outheights;
-    std::vector<ScenDev> scen;            // host copy at creation / host mirror for the sequential path
-    std::vector<uint32_t> tile_scen_h;
-    size_t capacity = 0;
-    uint32_t n_tiles = 0;
-    uint64_t total_steps = 0, steps_done = 0;
-    fpg_particles* pop = nullptr;
-    fpg_met* met = nullptr;
-    fpg_pbl* pbl = nullptr;
-    fpg_cellfield* wet = nullptr;
-    float4* ring = nullptr;               // n_frames * nodes packed (u,v,w,0)
-    fpg_surface_cell* sring = nullptr;    // n_frames * cells
-    float* pring = nullptr;               // n_frames * cells precipitation
-    float* staging = nullptr;             // 3 * nodes
-    BatchState* st = nullptr;
-    ScenDev* sc = nullptr;
-    uint32_t* tile_scen = nullptr;
-    uint2* items = nullptr;               // work items of the chosen launch shape
-    uint32_t n_items = 0;
-    size_t items_cap = 0;
-    uint32_t variant = 0;                 // index into kVariants
-    uint32_t resident[kNumVariants] = {}; // CTAs per SM of each shape (occupancy API)
-    float tuned_ms = 0.0f;
-    uint32_t* grid_counts = nullptr;
-    uint32_t* grid_mass = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    std::vector<uint32_t> released_h;     // host mirror of the release counts (sequential path)
-    std::vector<u32x4> counter_h;
-    int64_t t_h = 0;
-};
-
-static StepArgs make_step_args(fpg_batch* b) {
+StepArgs make_step_args(fpg_batch* b) {
     fpg_particles* P = b->pop;
     StepArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -393,7 +290,7 @@ static StepArgs make_step_args(fpg_batch* b) {
     return a;
 }
 
-static BatchConst make_const(const fpg_batch* b) {
+BatchConst make_const(const fpg_batch* b) {
     BatchConst c;
     c.start = b->cfg.start_seconds;
     c.frame_seconds = b->cfg.frame_seconds;
@@ -408,7 +305,7 @@ static BatchConst make_const(const fpg_batch* b) {
     return c;
 }
 
-static GridConst make_grid_const(const fpg_batch* b) {
+GridConst make_grid_const(const fpg_batch* b) {
     GridConst g;
     std::memset(&g, 0, sizeof(g));
     g.nx = b->cfg.out_nx; g.ny = b->cfg.out_ny; g.nz = b->cfg.out_nz;
@@ -420,7 +317,7 @@ static GridConst make_grid_const(const fpg_batch* b) {
     return g;
 }
 
-static PopFields pop_fields(fpg_batch* b) {
+PopFields pop_fields(fpg_batch* b) {
     PopFields F;
     for (int f = 0; f < FPG_FIELD_COUNT; ++f) F.f[f] = static_cast<uint32_t*>(b->pop->field[f]);
     return F;
@@ -428,7 +325,7 @@ static PopFields pop_fields(fpg_batch* b) {
 
 // The per-step kernels before and after the particle pass (shared by the
 // batched and sequential paths).
-static void enqueue_pre(fpg_batch* b, cudaStream_t s) {
+void enqueue_pre(fpg_batch* b, cudaStream_t s) {
     const BatchConst c = make_const(b);
     const uint32_t nodes = (uint32_t)(b->met->nx * b->met->ny * b->met->nz);
     const uint32_t cells = (uint32_t)(b->pbl->nx * b->pbl->ny);
@@ -442,22 +339,28 @@ static void enqueue_pre(fpg_batch* b, cudaStream_t s) {
     b->ctx->count(4);
 }
 
-static void enqueue_post(fpg_batch* b, cudaStream_t s) {
+void enqueue_post(fpg_batch* b, cudaStream_t s) {
     const BatchConst c = make_const(b);
     const GridConst g = make_grid_const(b);
     const size_t total = (size_t)g.cells * b->scen.size();
-    if (g.every) {
+    if (g.every && g.cells) {
         batch_grid_clear_kernel<<<b->ctx->sm_count * 4, 256, 0, s>>>(b->st, g.every, b->grid_counts, b->grid_mass,
                                                                      total);
         batch_grid_kernel<<<b->n_tiles, 256, 0, s>>>(b->st, b->sc, b->tile_scen, pop_fields(b), g, b->grid_counts,
                                                      b->grid_mass);
         b->ctx->count(2);
     }
+    if (b->inv) enqueue_inverse_sample(b, s);
     batch_end_kernel<<<1, 256, 0, s>>>(b->st, b->sc, c);
     b->ctx->count(1);
 }
 
-static void enqueue_step_kernel(fpg_batch* b, cudaStream_t s) {
+void enqueue_end(fpg_batch* b, cudaStream_t s) {
+    batch_end_kernel<<<1, 256, 0, s>>>(b->st, b->sc, make_const(b));
+    b->ctx->count(1);
+}
+
+void enqueue_step_kernel(fpg_batch* b, cudaStream_t s) {
     const StepVariant& v = kVariants[b->variant];
     const StepArgs a = make_step_args(b);
     const uint32_t grid = (uint32_t)b->ctx->sm_count * std::max(b->resident[b->variant], 1u);
@@ -465,14 +368,14 @@ static void enqueue_step_kernel(fpg_batch* b, cudaStream_t s) {
     b->ctx->count(1);
 }
 
-static void enqueue_batched_step(fpg_batch* b, cudaStream_t s) {
+void enqueue_batched_step(fpg_batch* b, cudaStream_t s) {
     enqueue_pre(b, s);
     enqueue_step_kernel(b, s);
     enqueue_post(b, s);
 }
 
 // Work items of shape `v`: every scenario cut into chunks of block * ppt slots.
-static fpg_status build_items(fpg_batch* b, uint32_t v) {
+fpg_status build_items(fpg_batch* b, uint32_t v) {
     const uint32_t chunk = kVariants[v].block * kVariants[v].ppt;
     std::vector<uint2> items;
     for (size_t s = 0; s < b->scen.size(); ++s)
@@ -494,6 +397,78 @@ static fpg_status build_items(fpg_batch* b, uint32_t v) {
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     return FPG_OK;
 }
+
+__global__ void __launch_bounds__(256) batch_pack_forced_kernel(const BatchState* st, const float4* __restrict__ ring,
+                                                                uint32_t nodes, float4* __restrict__ bracket) {
+    const float4* f0 = ring + (size_t)st->fa * nodes;
+    const float4* f1 = ring + (size_t)st->fb * nodes;
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < nodes; n += gridDim.x * blockDim.x) {
+        bracket[2u * n] = f0[n];
+        bracket[2u * n + 1u] = f1[n];
+    }
+}
+
+void enqueue_pack_forced(fpg_batch* b, cudaStream_t s) {
+    const uint32_t nodes = (uint32_t)(b->met->nx * b->met->ny * b->met->nz);
+    batch_pack_forced_kernel<<<b->ctx->sm_count * 4, 256, 0, s>>>(b->st, b->ring, nodes, b->met->bracket);
+    b->ctx->count(1);
+}
+
+fpg_status batch_reset(fpg_batch* b) {
+    cudaStream_t s = b->ctx->stream;
+    FPG_CUDA(cudaMemsetAsync(b->pop->block, 0, particles_block_bytes(b->capacity), s));
+    BatchState s0;
+    std::memset(&s0, 0, sizeof(s0));
+    s0.t = b->cfg.start_seconds;
+    FPG_CUDA(cudaMemcpyAsync(b->st, &s0, sizeof(s0), cudaMemcpyHostToDevice, s));
+    FPG_CUDA(cudaMemcpyAsync(b->sc, b->scen.data(), b->scen.size() * sizeof(ScenDev), cudaMemcpyHostToDevice, s));
+    FPG_CUDA(cudaStreamSynchronize(s));
+    b->steps_done = 0;
+    b->t_h = b->cfg.start_seconds;
+    for (size_t k = 0; k < b->scen.size(); ++k) {
+        b->released_h[k] = 0;
+        b->counter_h[k] = b->scen[k].counter;
+    }
+    return FPG_OK;
+}
+
+fpg_status ensure_graph(fpg_batch* b) {
+    if (b->exec) return FPG_OK;
+    cudaStream_t s = b->ctx->stream;
+    FPG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = b->ctx->launches.load();
+    enqueue_batched_step(b, s);
+    // capture launches nothing: take the count back, keep it per replay
+    b->graph_launches = b->ctx->launches.load() - before;
+    b->ctx->launches.fetch_sub(b->graph_launches);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess) return cuda_status(e);
+    b->graph = g;
+    FPG_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+    return FPG_OK;
+}
+
+// ReleaseError::OutOfGridDomain (release/mod.rs:41) of scenario d, checked at
+// the lattice's extreme points (lon, lat grow monotonically with the lattice
+// index, so every other point lies between them).
+fpg_status check_release_grid(const ScenDev& d, const fpg_grid_domain& g) {
+    const uint64_t ix_hi = std::min<uint64_t>(d.lat_nx - 1, d.count - 1);
+    const uint64_t iy_hi = std::min<uint64_t>(d.lat_nx - 1, (d.count - 1) / d.lat_nx);
+    for (int e = 0; e < 4; ++e) {
+        const uint64_t ix = (e & 1) ? ix_hi : 0, iy = (e & 2) ? iy_hi : 0;
+        const double lon = d.lon_min + (((double)ix + 0.5) / (double)d.lat_nx) * (d.lon_max - d.lon_min);
+        const double lat = d.lat_min + (((double)iy + 0.5) / (double)d.lat_nx) * (d.lat_max - d.lat_min);
+        const double x = (lon - g.xlon0) / g.dx;
+        const double y = (lat - g.ylat0) / g.dy;
+        if (!(x >= 0.0 && x < (double)(g.nx - 1) && y >= 0.0 && y < (double)(g.ny - 1))) return FPG_ERR_OUT_OF_GRID;
+    }
+    return FPG_OK;
+}
+
+}  // namespace fpg
+
+using namespace fpg;
 
 extern "C" fpg_status fpg_batch_destroy(fpg_batch* b) {
     if (!b) return FPG_OK;
@@ -552,22 +527,9 @@ extern "C" fpg_status fpg_batch_create(fpg_ctx* ctx, const fpg_batch_config* cfg
         d.lat_nxy = d.lat_nx * d.lat_nx > 0 ? d.lat_nx * d.lat_nx : 1;
         d.lat_nz = (r.particle_count + d.lat_nxy - 1) / d.lat_nxy;
         if (d.lat_nz < 1) d.lat_nz = 1;
-        // ReleaseError::OutOfGridDomain (release/mod.rs:41) checked at the
-        // lattice's extreme points (lon, lat grow monotonically with the
-        // lattice index, so every other point lies between them)
-        const uint64_t ix_hi = std::min<uint64_t>(d.lat_nx - 1, d.count - 1);
-        const uint64_t iy_hi = std::min<uint64_t>(d.lat_nx - 1, (d.count - 1) / d.lat_nx);
-        for (int e = 0; e < 4; ++e) {
-            const uint64_t ix = (e & 1) ? ix_hi : 0, iy = (e & 2) ? iy_hi : 0;
-            const double lon = r.lon_min + (((double)ix + 0.5) / (double)d.lat_nx) * (r.lon_max - r.lon_min);
-            const double lat = r.lat_min + (((double)iy + 0.5) / (double)d.lat_nx) * (r.lat_max - r.lat_min);
-            const double x = (lon - cfg->release_grid.xlon0) / cfg->release_grid.dx;
-            const double y = (lat - cfg->release_grid.ylat0) / cfg->release_grid.dy;
-            if (!(x >= 0.0 && x < (double)(cfg->release_grid.nx - 1) && y >= 0.0 &&
-                  y < (double)(cfg->release_grid.ny - 1))) {
-                delete b;
-                return FPG_ERR_OUT_OF_GRID;
-            }
+        if (check_release_grid(d, cfg->release_grid) != FPG_OK) {
+            delete b;
+            return FPG_ERR_OUT_OF_GRID;
         }
         b->scen.push_back(d);
         for (uint32_t t = 0; t < d.n_tiles; ++t) b->tile_scen_h.push_back((uint32_t)s);
@@ -660,19 +622,14 @@ extern "C" fpg_status fpg_batch_run(fpg_batch* b, uint32_t n_steps, int32_t use_
     if (b->steps_done >= b->total_steps) return FPG_ERR_SIMULATION_COMPLETE;
     const uint64_t n = std::min<uint64_t>(n_steps, b->total_steps - b->steps_done);
     cudaStream_t s = b->ctx->stream;
-    if (use_graph && !b->exec) {
-        FPG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        enqueue_batched_step(b, s);
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamEndCapture(s, &g);
-        if (e != cudaSuccess) return cuda_status(e);
-        b->graph = g;
-        FPG_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+    if (use_graph) {
+        const fpg_status st = ensure_graph(b);
+        if (st != FPG_OK) return st;
     }
     for (uint64_t i = 0; i < n; ++i) {
         if (use_graph) {
             FPG_CUDA(cudaGraphLaunch(b->exec, s));
-            b->ctx->count(b->cfg.output_every_steps ? 8 : 6);
+            b->ctx->count(b->graph_launches);
         } else {
             enqueue_batched_step(b, s);
             FPG_CHECK_LAUNCH();

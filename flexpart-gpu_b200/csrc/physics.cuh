@@ -69,36 +69,58 @@ __device__ __forceinline__ float2 box_muller(float u0, float u1) {
     return make_float2(radius * cosf(theta), radius * sinf(theta));
 }
 
+// ---- scalar helpers of the templated physics --------------------------------
+// The Hanna and Langevin routines below are templates over the scalar type:
+// float for the step itself, and the dual number of the adjoint (dual.cuh),
+// which carries derivatives beside the value and supplies the same helper
+// names.  For float every helper is the plain CUDA call, so the float
+// instantiation performs exactly the operations written, in the same order.
+__device__ __forceinline__ float val(float x) { return x; }
+__device__ __forceinline__ float xexp(float x) { return expf(x); }
+__device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ float xcbrt(float x) { return pow_third(x); }
+__device__ __forceinline__ float xpow(float x, float e) { return powf(x, e); }
+__device__ __forceinline__ float xmax(float x, float c) { return fmaxf(x, c); }
+__device__ __forceinline__ float xclamp(float x, float lo, float hi) { return clampf(x, lo, hi); }
+__device__ __forceinline__ float xabs(float x) { return fabsf(x); }
+
 // ---- Hanna (physics/hanna.rs:49-163, langevin_fused.wgsl:224-293) ----------
 // Stability branch of hanna.rs:69-112: 0 neutral, 1 unstable, 2 stable.
 enum { REGIME_NEUTRAL = 0, REGIME_UNSTABLE = 1, REGIME_STABLE = 2 };
 
-struct Hanna {
+template <class T>
+struct HannaT {
     float ust, wst, ol, h;
-    float sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
+    T sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
     int regime;
 };
+using Hanna = HannaT<float>;
 
 __device__ __forceinline__ float obukhov_from_inverse(float oli) {
     // hanna.rs:169-174: |1/L| < 1e-5 is neutral (L = +inf).
     return fabsf(oli) < 1.0e-5f ? __int_as_float(0x7f800000) : 1.0f / oli;
 }
 
-__device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float ol, float h_in, float z_in) {
-    Hanna o;
+__device__ __forceinline__ int hanna_regime(float ol, float h) {
+    return (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) ? REGIME_NEUTRAL
+           : ol < 0.0f                                         ? REGIME_UNSTABLE
+                                                               : REGIME_STABLE;
+}
+
+template <class T>
+__device__ __forceinline__ HannaT<T> compute_hanna_t(float ust_in, float wst_in, float ol, float h_in, T z_in) {
+    HannaT<T> o;
     const float ust = fmaxf(ust_in, 1.0e-4f);
     const float wst = fmaxf(wst_in, 0.0f);
     const float h = fmaxf(h_in, 1.0f);
-    const float z = clampf(z_in, 0.0f, h);
-    const float zeta = clampf(z / h, 0.0f, 1.0f);
-    float sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
-    o.regime = (!finitef(ol) || ol == 0.0f || h / fabsf(ol) < 1.0f) ? REGIME_NEUTRAL
-               : ol < 0.0f                                         ? REGIME_UNSTABLE
-                                                                   : REGIME_STABLE;
+    const T z = xclamp(z_in, 0.0f, h);
+    const T zeta = xclamp(z / h, 0.0f, 1.0f);
+    T sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
+    o.regime = hanna_regime(ol, h);
     if (o.regime == REGIME_NEUTRAL) {
-        const float corr = z / ust;
-        sigu = 1.0e-2f + 2.0f * ust * expf(-3.0e-4f * corr);
-        sigw = 1.3f * ust * expf(-2.0e-4f * corr);
+        const T corr = z / ust;
+        sigu = 1.0e-2f + 2.0f * ust * xexp(-3.0e-4f * corr);
+        sigw = 1.3f * ust * xexp(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
         sigv = sigw;
@@ -106,43 +128,47 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
         tlv = tlu;
         tlw = tlu;
     } else if (o.regime == REGIME_UNSTABLE) {
-        sigu = 1.0e-2f + ust * pow_third(12.0f - 0.5f * h / ol);
+        sigu = T(1.0e-2f + ust * pow_third(12.0f - 0.5f * h / ol));
         sigv = sigu;
-        const float c = pow_third(zeta);
-        const float z23 = c * c;
-        const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
-        sigw = sqrtf(sigw_sq) + 1.0e-2f;
-        const float zm13 = 1.0f / (zeta >= 1.0e-3f ? c : pow_third(1.0e-3f));
+        const T c = xcbrt(zeta);
+        const T z23 = c * c;
+        const T sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
+        sigw = xsqrt(sigw_sq) + 1.0e-2f;
+        const T zm13 = 1.0f / (val(zeta) >= 1.0e-3f ? c : T(pow_third(1.0e-3f)));
         dsigwdz = 0.5f / sigw / h * (-1.4f * ust * ust + wst * wst * (0.8f * zm13 - 1.8f * z23));
-        tlu = 0.15f * h / sigu;
+        tlu = T(0.15f * h / val(sigu));
         tlv = tlu;
-        if (z < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * fabsf(z / ol)));
-        else if (zeta < 0.1f) tlw = 0.59f * z / sigw;
-        else tlw = 0.15f * h / sigw * (1.0f - expf(-5.0f * zeta));
+        if (val(z) < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * xabs(z / ol)));
+        else if (val(zeta) < 0.1f) tlw = 0.59f * z / sigw;
+        else tlw = 0.15f * h / sigw * (1.0f - xexp(-5.0f * zeta));
     } else {
         sigu = 1.0e-2f + 2.0f * ust * (1.0f - zeta);
         sigv = 1.0e-2f + 1.3f * ust * (1.0f - zeta);
         sigw = sigv;
-        dsigwdz = -1.3f * ust / h;
-        tlu = 0.15f * h / sigu * sqrtf(zeta);
+        dsigwdz = T(-1.3f * ust / h);
+        tlu = 0.15f * h / sigu * xsqrt(zeta);
         tlv = 0.467f * tlu;
-        tlw = 0.1f * h / sigw * powf(zeta, 0.8f);
+        tlw = 0.1f * h / sigw * xpow(zeta, 0.8f);
     }
-    tlu = fmaxf(tlu, 10.0f);
-    tlv = fmaxf(tlv, 10.0f);
-    tlw = fmaxf(tlw, 30.0f);
-    if (dsigwdz == 0.0f) dsigwdz = 1.0e-10f;
-    if (!finitef(sigu) || sigu <= 0.0f) sigu = 1.0e-2f;
-    if (!finitef(sigv) || sigv <= 0.0f) sigv = 1.0e-2f;
-    if (!finitef(sigw) || sigw <= 0.0f) sigw = 1.0e-2f;
-    if (!finitef(tlu)) tlu = 10.0f;
-    if (!finitef(tlv)) tlv = 10.0f;
-    if (!finitef(tlw)) tlw = 30.0f;
-    if (!finitef(dsigwdz)) dsigwdz = 1.0e-10f;
+    tlu = xmax(tlu, 10.0f);
+    tlv = xmax(tlv, 10.0f);
+    tlw = xmax(tlw, 30.0f);
+    if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
+    if (!finitef(val(sigu)) || val(sigu) <= 0.0f) sigu = T(1.0e-2f);
+    if (!finitef(val(sigv)) || val(sigv) <= 0.0f) sigv = T(1.0e-2f);
+    if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
+    if (!finitef(val(tlu))) tlu = T(10.0f);
+    if (!finitef(val(tlv))) tlv = T(10.0f);
+    if (!finitef(val(tlw))) tlw = T(30.0f);
+    if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
     o.ust = ust; o.wst = wst; o.ol = ol; o.h = h;
     o.sigu = sigu; o.sigv = sigv; o.sigw = sigw; o.dsigwdz = dsigwdz;
     o.tlu = tlu; o.tlv = tlv; o.tlw = tlw;
     return o;
+}
+
+__device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float ol, float h_in, float z_in) {
+    return compute_hanna_t<float>(ust_in, wst_in, ol, h_in, z_in);
 }
 
 // hanna_short_w (langevin_fused.wgsl:296-344): sigw, dsigwdz, tlw at a new
@@ -150,41 +176,47 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
 // The branch test of the shader (`!finite(ol) || ol == 0 || h/|ol| < 1`,
 // then `ol < 0`) sees the same floored h and the same ol as compute_hanna's
 // for this particle, so its outcome is the `regime` compute_hanna found.
-__device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float ol, float h_in, float z_in,
-                                              int regime, float& sigw_o, float& dsigwdz_o, float& tlw_o) {
+template <class T>
+__device__ __forceinline__ void hanna_short_w_t(float ust_in, float wst_in, float ol, float h_in, T z_in, int regime,
+                                                T& sigw_o, T& dsigwdz_o, T& tlw_o) {
     const float ust = fmaxf(ust_in, 1.0e-4f);
     const float wst = fmaxf(wst_in, 0.0f);
     const float h = fmaxf(h_in, 1.0f);
-    const float z = clampf(z_in, 0.0f, h);
-    const float zeta = clampf(z / h, 0.0f, 1.0f);
-    float sigw, dsigwdz, tlw;
+    const T z = xclamp(z_in, 0.0f, h);
+    const T zeta = xclamp(z / h, 0.0f, 1.0f);
+    T sigw, dsigwdz, tlw;
     if (regime == REGIME_NEUTRAL) {
-        const float corr = z / ust;
-        sigw = 1.3f * ust * expf(-2.0e-4f * corr);
+        const T corr = z / ust;
+        sigw = 1.3f * ust * xexp(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
         tlw = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
     } else if (regime == REGIME_UNSTABLE) {
-        const float c = pow_third(zeta);
-        const float z23 = c * c;
-        const float sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
-        sigw = sqrtf(sigw_sq) + 1.0e-2f;
-        const float zm13 = 1.0f / (zeta >= 1.0e-3f ? c : pow_third(1.0e-3f));
+        const T c = xcbrt(zeta);
+        const T z23 = c * c;
+        const T sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
+        sigw = xsqrt(sigw_sq) + 1.0e-2f;
+        const T zm13 = 1.0f / (val(zeta) >= 1.0e-3f ? c : T(pow_third(1.0e-3f)));
         dsigwdz = 0.5f / sigw / h * (-1.4f * ust * ust + wst * wst * (0.8f * zm13 - 1.8f * z23));
-        if (z < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * fabsf(z / ol)));
-        else if (zeta < 0.1f) tlw = 0.59f * z / sigw;
-        else tlw = 0.15f * h / sigw * (1.0f - expf(-5.0f * zeta));
+        if (val(z) < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * xabs(z / ol)));
+        else if (val(zeta) < 0.1f) tlw = 0.59f * z / sigw;
+        else tlw = 0.15f * h / sigw * (1.0f - xexp(-5.0f * zeta));
     } else {
         sigw = 1.0e-2f + 1.3f * ust * (1.0f - zeta);
-        dsigwdz = -1.3f * ust / h;
-        tlw = 0.1f * h / sigw * powf(zeta, 0.8f);
+        dsigwdz = T(-1.3f * ust / h);
+        tlw = 0.1f * h / sigw * xpow(zeta, 0.8f);
     }
-    tlw = fmaxf(tlw, 30.0f);
-    if (dsigwdz == 0.0f) dsigwdz = 1.0e-10f;
-    if (!finitef(sigw) || sigw <= 0.0f) sigw = 1.0e-2f;
-    if (!finitef(tlw)) tlw = 30.0f;
-    if (!finitef(dsigwdz)) dsigwdz = 1.0e-10f;
+    tlw = xmax(tlw, 30.0f);
+    if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
+    if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
+    if (!finitef(val(tlw))) tlw = T(30.0f);
+    if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
     sigw_o = sigw; dsigwdz_o = dsigwdz; tlw_o = tlw;
+}
+
+__device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float ol, float h_in, float z_in,
+                                              int regime, float& sigw_o, float& dsigwdz_o, float& tlw_o) {
+    hanna_short_w_t<float>(ust_in, wst_in, ol, h_in, z_in, regime, sigw_o, dsigwdz_o, tlw_o);
 }
 
 // The Langevin updates below take Hanna outputs only: sigma >= 0.01 and
@@ -193,30 +225,40 @@ __device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float 
 // (physics/langevin.rs:116-121,146-150) are the identity and are omitted.
 
 // ---- Langevin OU updates (physics/langevin.rs:116-170, langevin_fused.wgsl:350-389)
-__device__ __forceinline__ float langevin_h(float prev, float sigma, float tl, float dt, float eta) {
-    const float ratio = dt / tl;
-    float next;
-    if (ratio < 0.5f) {
-        next = (1.0f - ratio) * prev + eta * sigma * sqrtf(fmaxf(2.0f * ratio, 0.0f));
+template <class T>
+__device__ __forceinline__ T langevin_h_t(T prev, T sigma, T tl, float dt, float eta) {
+    const T ratio = dt / tl;
+    T next;
+    if (val(ratio) < 0.5f) {
+        next = (1.0f - ratio) * prev + eta * sigma * xsqrt(xmax(2.0f * ratio, 0.0f));
     } else {
-        const float corr = expf(-ratio);
-        next = corr * prev + eta * sigma * sqrtf(fmaxf(1.0f - corr * corr, 0.0f));
+        const T corr = xexp(-ratio);
+        next = corr * prev + eta * sigma * xsqrt(xmax(1.0f - corr * corr, 0.0f));
     }
-    return finitef(next) ? next : 0.0f;
+    return finitef(val(next)) ? next : T(0.0f);
+}
+
+template <class T>
+__device__ __forceinline__ T langevin_v_t(T prev, T sigma_w, T tlw, T dsigwdz, float dt, float rho, float eta) {
+    const T drift = sigma_w * (dsigwdz + rho * sigma_w);
+    const T ratio = dt / tlw;
+    T next;
+    if (val(ratio) < 0.5f) {
+        next = (1.0f - ratio) * prev + eta * sigma_w * xsqrt(xmax(2.0f * ratio, 0.0f)) + dt * drift;
+    } else {
+        const T corr = xexp(-ratio);
+        next = corr * prev + eta * sigma_w * xsqrt(xmax(1.0f - corr * corr, 0.0f)) + tlw * (1.0f - corr) * drift;
+    }
+    return finitef(val(next)) ? next : T(0.0f);
+}
+
+__device__ __forceinline__ float langevin_h(float prev, float sigma, float tl, float dt, float eta) {
+    return langevin_h_t<float>(prev, sigma, tl, dt, eta);
 }
 
 __device__ __forceinline__ float langevin_v(float prev, float sigma_w, float tlw, float dsigwdz, float dt,
                                             float rho, float eta) {
-    const float drift = sigma_w * (dsigwdz + rho * sigma_w);
-    const float ratio = dt / tlw;
-    float next;
-    if (ratio < 0.5f) {
-        next = (1.0f - ratio) * prev + eta * sigma_w * sqrtf(fmaxf(2.0f * ratio, 0.0f)) + dt * drift;
-    } else {
-        const float corr = expf(-ratio);
-        next = corr * prev + eta * sigma_w * sqrtf(fmaxf(1.0f - corr * corr, 0.0f)) + tlw * (1.0f - corr) * drift;
-    }
-    return finitef(next) ? next : 0.0f;
+    return langevin_v_t<float>(prev, sigma_w, tlw, dsigwdz, dt, rho, eta);
 }
 
 // ---- Deposition --------------------------------------------------------------

@@ -5,6 +5,7 @@
 
 #include "fpg_internal.h"
 #include "physics.cuh"
+#include "dual.cuh"
 
 namespace fpg {
 
@@ -143,9 +144,64 @@ __device__ __forceinline__ void split_coord(float coord, uint32_t n, int32_t& ce
     frac = f;
 }
 
-__device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_heights, uint32_t p,
-                                              uint32_t rng_index, float alpha, u32x4 counter, uint32_t key0,
-                                              uint32_t key1) {
+// Turbulence of one particle (langevin_fused.wgsl:414-515 after the PBL
+// lookup and the noise draws): Hanna at the particle height, horizontal
+// Langevin updates, then the vertical sub-steps with ground and PBL-top
+// reflection.  A template over the scalar type: float for the step, the
+// dual number of the adjoint for its Jacobian (same values, bit for bit).
+template <class T>
+__device__ __forceinline__ void turbulence_update(const StepArgs& a, float4 cell, float2 e_uv, float2 e_w01,
+                                                  float2 e_w23, T& pz, T& tu, T& tv, T& tw, int32_t& cbt) {
+    const HannaT<T> hn = compute_hanna_t<T>(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
+    tu = langevin_h_t<T>(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
+    tv = langevin_h_t<T>(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
+    if (a.n_sub == 0u) {
+        tw = langevin_v_t<T>(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
+        return;
+    }
+    const float dt_sub = a.tdt / (float)a.n_sub;
+    const float h = hn.h;
+    const float zmin = a.zmin;
+    T sigw = hn.sigw, dsigwdz = hn.dsigwdz, tlw = hn.tlw;
+    for (uint32_t sub = 0; sub < a.n_sub; ++sub) {
+        const float eta = sub == 0u ? e_w01.x : sub == 1u ? e_w01.y : sub == 2u ? e_w23.x : e_w23.y;
+        tw = langevin_v_t<T>(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
+        pz = pz + tw * dt_sub;
+        if (h > zmin) {
+            T z = pz;
+            for (int bounce = 0; bounce < 10; ++bounce) {
+                if (val(z) < zmin) { z = 2.0f * zmin - z; cbt = -cbt; tw = -tw; }
+                else if (val(z) > h) { z = 2.0f * h - z; cbt = -cbt; tw = -tw; }
+                else break;
+            }
+            pz = xclamp(z, zmin, h);
+        }
+        if (sub < a.n_sub - 1u) hanna_short_w_t<T>(hn.ust, hn.wst, hn.ol, hn.h, pz, hn.regime, sigw, dsigwdz, tlw);
+    }
+}
+
+// What the step records for its adjoint (a policy of particle_step): NoTape
+// records nothing and keeps the plain float path.
+struct NoTape {
+    static constexpr bool on = false;
+    __device__ __forceinline__ void advect(uint32_t, float, float, float, float, float, float, uint32_t) {}
+    __device__ __forceinline__ void turb(uint32_t, float, float, float, float, float, float, float, float) {}
+    __device__ __forceinline__ void deposit(uint32_t, float) {}
+    __device__ __forceinline__ void out(uint32_t, float, float, float, float) {}
+};
+
+// Clamp states of the advection, one bit each: set when the raw value lies
+// strictly inside its clamp range (the clamp passes the derivative).
+enum : uint32_t { ADV_PX = 1u, ADV_PY = 2u, ADV_PZ = 4u, ADV_X1 = 8u, ADV_Y1 = 16u, ADV_Z1 = 32u };
+
+__device__ __forceinline__ uint32_t inside(float v, float lo, float hi, uint32_t bit) {
+    return (v > lo && v < hi) ? bit : 0u;
+}
+
+template <class Tape>
+__device__ __forceinline__ void particle_step_t(const StepArgs& a, const float* s_heights, uint32_t p,
+                                                uint32_t rng_index, float alpha, u32x4 counter, uint32_t key0,
+                                                uint32_t key1, Tape& tape) {
     const bool dry_on = (a.stages & FPG_STAGE_DRY) && a.dry_mode != FPG_FORCING_NONE;
     const bool wet_on = (a.stages & FPG_STAGE_WET) && a.wet_mode != FPG_FORCING_NONE;
     if (!(a.flags[p] & FLAG_ACTIVE)) {
@@ -167,15 +223,27 @@ __device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_
         const float u0 = s0.x + tu, v0 = s0.y + tv, w0 = s0.z;
         const float xmax = (float)(a.nx - 1u), ymax = (float)(a.ny - 1u);
         const float ztop = a.has_heights ? s_heights[a.nz - 1u] : (float)(a.nz - 1u);
-        const float pxp = clampf(x0 + (u0 * a.xs) * a.dt, 0.0f, xmax);
-        const float pyp = clampf(y0 + (v0 * a.ys) * a.dt, 0.0f, ymax);
-        const float pzp = clampf(z0 + (w0 * a.zs) * a.dt, 0.0f, ztop);
+        const float rxp = x0 + (u0 * a.xs) * a.dt;
+        const float ryp = y0 + (v0 * a.ys) * a.dt;
+        const float rzp = z0 + (w0 * a.zs) * a.dt;
+        const float pxp = clampf(rxp, 0.0f, xmax);
+        const float pyp = clampf(ryp, 0.0f, ymax);
+        const float pzp = clampf(rzp, 0.0f, ztop);
         const float3 s1 = sample_dual(a, s_heights, pxp, pyp, pzp, alpha);
         const float u1 = s1.x + tu, v1 = s1.y + tv, w1 = s1.z;
         const float cu = 0.5f * (u0 + u1), cv = 0.5f * (v0 + v1), cw = 0.5f * (w0 + w1);
-        const float x1 = clampf(x0 + (cu * a.xs) * a.dt, 0.0f, xmax);
-        const float y1 = clampf(y0 + (cv * a.ys) * a.dt, 0.0f, ymax);
-        pz = clampf(z0 + (cw * a.zs) * a.dt, 0.0f, ztop);
+        const float rx1 = x0 + (cu * a.xs) * a.dt;
+        const float ry1 = y0 + (cv * a.ys) * a.dt;
+        const float rz1 = z0 + (cw * a.zs) * a.dt;
+        const float x1 = clampf(rx1, 0.0f, xmax);
+        const float y1 = clampf(ry1, 0.0f, ymax);
+        pz = clampf(rz1, 0.0f, ztop);
+        if constexpr (Tape::on) {
+            const uint32_t fl = inside(rxp, 0.0f, xmax, ADV_PX) | inside(ryp, 0.0f, ymax, ADV_PY) |
+                                inside(rzp, 0.0f, ztop, ADV_PZ) | inside(rx1, 0.0f, xmax, ADV_X1) |
+                                inside(ry1, 0.0f, ymax, ADV_Y1) | inside(rz1, 0.0f, ztop, ADV_Z1);
+            tape.advect(p, x0, y0, z0, pxp, pyp, pzp, fl);
+        }
         split_coord(x1, a.nx, cx, px);
         split_coord(y1, a.ny, cy, py);
         a.cell_x[p] = cx; a.cell_y[p] = cy;
@@ -190,7 +258,6 @@ __device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_
         const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(a.pnx - 1u)));
         const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(a.pny - 1u)));
         const float4 cell = __ldg(a.pbl + (i * a.pny + j));
-        const Hanna hn = compute_hanna(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
 
         const uint32_t n_vert = a.n_sub > 1u ? a.n_sub : 1u;
         const uint32_t blocks = (2u + n_vert + 3u) / 4u;
@@ -201,40 +268,26 @@ __device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_
         const float2 e_w01 = box_muller(u32_to_uniform01(b0.z), u32_to_uniform01(b0.w));
         const float2 e_w23 = box_muller(u32_to_uniform01(b1.x), u32_to_uniform01(b1.y));
 
-        tu = langevin_h(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
-        tv = langevin_h(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
         float tw = a.turb_w[p];
-        if (a.n_sub == 0u) {
-            tw = langevin_v(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
+        const int32_t cbt_in = a.n_sub == 0u ? 0 : a.cbt[p];
+        int32_t cbt = cbt_in;
+        if constexpr (Tape::on) {
+            // tangents: .a along the height after advection (and, for tu/tv,
+            // .b along their own input); .b of z and tw along the input tw
+            D2 zd(pz, 1.0f, 0.0f), ud(tu, 0.0f, 1.0f), vd(tv, 0.0f, 1.0f), wd(tw, 0.0f, 1.0f);
+            turbulence_update<D2>(a, cell, e_uv, e_w01, e_w23, zd, ud, vd, wd, cbt);
+            tape.turb(p, zd.a, zd.b, wd.a, wd.b, ud.a, ud.b, vd.a, vd.b);
+            pz = zd.v; tu = ud.v; tv = vd.v; tw = wd.v;
         } else {
-            int32_t cbt = a.cbt[p];
-            const int32_t cbt_in = cbt;
-            const float dt_sub = a.tdt / (float)a.n_sub;
-            const float h = hn.h;
-            const float zmin = a.zmin;
-            float sigw = hn.sigw, dsigwdz = hn.dsigwdz, tlw = hn.tlw;
-            for (uint32_t sub = 0; sub < a.n_sub; ++sub) {
-                const float eta = sub == 0u ? e_w01.x : sub == 1u ? e_w01.y : sub == 2u ? e_w23.x : e_w23.y;
-                tw = langevin_v(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
-                pz = pz + tw * dt_sub;
-                if (h > zmin) {
-                    float z = pz;
-                    for (int bounce = 0; bounce < 10; ++bounce) {
-                        if (z < zmin) { z = 2.0f * zmin - z; cbt = -cbt; tw = -tw; }
-                        else if (z > h) { z = 2.0f * h - z; cbt = -cbt; tw = -tw; }
-                        else break;
-                    }
-                    pz = clampf(z, zmin, h);
-                }
-                if (sub < a.n_sub - 1u) hanna_short_w(hn.ust, hn.wst, hn.ol, hn.h, pz, hn.regime, sigw, dsigwdz, tlw);
-            }
-            if (cbt != cbt_in) a.cbt[p] = cbt;
+            turbulence_update<float>(a, cell, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
         }
+        if (a.n_sub != 0u && cbt != cbt_in) a.cbt[p] = cbt;
         a.turb_u[p] = tu; a.turb_v[p] = tv; a.turb_w[p] = tw;
     }
     if ((a.stages & FPG_STAGE_ADVECT) || (turb_on && a.n_sub != 0u)) a.pos_z[p] = pz;
 
     // ---- dry_deposition.wgsl:89-105 and wet_deposition.wgsl:203-216 ----
+    float surv_total = 1.0f;
     if (dry_on || wet_on) {
         float survival = 1.0f;
         if (dry_on) {
@@ -274,7 +327,19 @@ __device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_
             if (wet_on) m = m * wsurv;
             a.mass[k][p] = m;
         }
+        if constexpr (Tape::on) surv_total = (dry_on && !(pz >= 2.0f * a.href) ? survival : 1.0f) * wsurv;
     }
+    if constexpr (Tape::on) {
+        tape.deposit(p, surv_total);
+        tape.out(p, (float)cx + px, (float)cy + py, pz, a.mass[0][p]);
+    }
+}
+
+__device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_heights, uint32_t p,
+                                              uint32_t rng_index, float alpha, u32x4 counter, uint32_t key0,
+                                              uint32_t key1) {
+    NoTape t;
+    particle_step_t<NoTape>(a, s_heights, p, rng_index, alpha, counter, key0, key1, t);
 }
 
 

@@ -130,6 +130,15 @@ _sig("fpg_batch_tuning_candidates", _u32, _vp, _u32)
 _sig("fpg_batch_autotune", _i32, _vp, _u32, _vp, _u32, _vp)
 _sig("fpg_batch_set_tuning", _i32, _vp, _vp)
 _sig("fpg_batch_get_tuning", _i32, _vp, _vp)
+_sig("fpg_inverse_create", _i32, _vp, _vp, _vp, _vp, _sz, _sz, _sz, _sz, _vp, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_inverse_destroy", _i32, _vp)
+_sig("fpg_inverse_upload_frame", _i32, _vp, _u32, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_inverse_set_sources", _i32, _vp, _vp, _vp)
+_sig("fpg_inverse_set_wind_bias", _i32, _vp, _vp)
+_sig("fpg_inverse_forward", _i32, _vp, _vp)
+_sig("fpg_inverse_backward", _i32, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_inverse_batch", _vp, _vp)
+_sig("fpg_inverse_device_bytes", ctypes.c_uint64, _vp)
 _sig("fpg_sorter_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
 _sig("fpg_sorter_destroy", _i32, _vp)
 _sig("fpg_sort_by_cell", _i32, _vp, _vp, _vp, _vp, _vp, _vp)
@@ -172,4 +181,11 @@ EXPORTED_DRIVER = [
     "fpg_batch_steps_done", "fpg_batch_scenario_slots", "fpg_batch_particles", "fpg_batch_download_grids",
     "fpg_batch_errors", "fpg_batch_tuning_candidates", "fpg_batch_autotune", "fpg_batch_set_tuning",
     "fpg_batch_get_tuning",
+]
+
+# Every symbol include/fpg_adjoint.h declares.
+EXPORTED_ADJOINT = [
+    "fpg_inverse_create", "fpg_inverse_destroy", "fpg_inverse_upload_frame", "fpg_inverse_set_sources",
+    "fpg_inverse_set_wind_bias", "fpg_inverse_forward", "fpg_inverse_backward", "fpg_inverse_batch",
+    "fpg_inverse_device_bytes",
 ]

@@ -207,6 +207,20 @@ class BatchTuning(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Receptor(ctypes.Structure):
+    """``fpg_receptor`` (include/fpg_adjoint.h)."""
+
+    _fields_ = [("instance", ctypes.c_uint32), ("i", ctypes.c_uint32), ("j", ctypes.c_uint32)]
+
+
+class InverseConfig(ctypes.Structure):
+    """``fpg_inverse_config`` (include/fpg_adjoint.h)."""
+
+    _fields_ = [("batch", BatchConfig), ("sample_every_steps", ctypes.c_uint32),
+                ("receptor_top_m", ctypes.c_float), ("receptor_ramp_m", ctypes.c_float),
+                ("checkpoint_every", ctypes.c_uint32)]
+
+
 class MetBracket(ctypes.Structure):
     """``fpg_met_bracket``: MetTimeBracket (timeloop.rs:270-285)."""
 

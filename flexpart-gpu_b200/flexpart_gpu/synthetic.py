@@ -297,3 +297,66 @@ def config2(n_scenarios: int = 256, lo: int = 10_000, hi: int = 1_000_000, hours
         keys.append((int(rng.integers(0, 2**32)), s))
     return Ensemble("config2", met, sources, keys, start=t0, end=end, dt=dt, out_shape=(met.nx, met.ny, 3),
                     outheights=[100.0, 500.0, 1000.0])
+
+
+@dataclass
+class Inversion:
+    """A source-inversion problem: sources (one batch scenario each, own key),
+    receptors (cells of the lowest layer), observations."""
+
+    name: str
+    ensemble: Ensemble         # sources as scenarios, with their true masses
+    receptors: list            # (instance, i, j)
+    instance: list             # instance of each source
+    sample_every: int = 12
+    receptor_top_m: float = 100.0
+    receptor_ramp_m: float = 20.0
+    checkpoint_every: int = 8
+
+
+def config3(n_particles: int = 1_000_000, n_sources: int = 16, n_receptors: int = 200, hours: int = 24,
+            met: MetSpec | None = None, seed: int = 3, smooth: bool = False) -> Inversion:
+    """Source inversion on the configuration-0 met (90x60 at 0.5 deg x 20
+    levels, 2 frames 3 h apart, cycled): n_sources point sources at heights
+    U(10, 300) m with 1 kg each, released over 6 h from a step in the first
+    half of the run, n_particles in all (equal shares), their own Philox
+    keys; n_receptors distinct random cells of the lowest layer (0-100 m),
+    sampled every 3 h; dt 900 s.  smooth=True makes the PBL inputs uniform
+    in space and switches deposition off, so the forward map has no
+    discontinuity in position (for finite-difference checks)."""
+    if met is None:
+        met = MetSpec(nx=90, ny=60, nz=20, dx_deg=0.5, dy_deg=0.5, xlon0=-10.0, ylat0=35.0, n_frames=2, seed=0)
+    rng = np.random.default_rng(300 + seed)
+    t0 = EPOCH_2024
+    dt = 900
+    end = t0 + hours * 3600
+    per = n_particles // n_sources
+    sources, keys = [], []
+    half_steps = max((end - t0) // dt // 2, 1)
+    lon_span = (met.nx - 1) * met.dx_deg
+    lat_span = (met.ny - 1) * met.dy_deg
+    for s in range(n_sources):
+        lon = float(met.xlon0 + rng.uniform(0.25, 0.75) * lon_span)
+        lat = float(met.ylat0 + rng.uniform(0.25, 0.75) * lat_span)
+        z = float(rng.uniform(10.0, 300.0))
+        start = int(t0 + dt * int(rng.integers(0, half_steps)))
+        sources.append(Source(lon=lon, lat=lat, z_min=z, z_max=z, mass_kg=1.0,
+                              particle_count=per + (1 if s < n_particles - per * n_sources else 0),
+                              start=start, end=min(start + 6 * 3600, end)))
+        keys.append((int(rng.integers(0, 2**32)), 1000 + s))
+    cells = rng.choice(met.nx * met.ny, size=n_receptors, replace=False)
+    receptors = [(0, int(c // met.ny), int(c % met.ny)) for c in cells]
+    ens = Ensemble("config3", met, sources, keys, start=t0, end=end, dt=dt, out_shape=(met.nx, met.ny, 1),
+                   outheights=[100.0], dry_velocity=0.0 if smooth else 0.002)
+    inv = Inversion("config3", ens, receptors, [0] * n_sources)
+    inv.smooth = smooth
+    return inv
+
+
+def make_frames_uniform_pbl(spec: MetSpec):
+    """make_frames with every surface cell replaced by the first cell's
+    values (spatially uniform PBL inputs)."""
+    frames = make_frames(spec)
+    for f in frames:
+        f["surface"][:] = f["surface"][0]
+    return frames

@@ -353,7 +353,7 @@ def pbl_diagnostics(surface_t0, surface_t1, alpha, nx, ny, options=None, dtype=n
 
 def step(state: State, n, met, pbl: Pbl, params: StepParams, wet_cells_lf=None, wet_shape=None,
          threads=0, dry_velocity=None, wet_lambda=None, wet_fraction=None,
-         dry_prob=None, wet_prob=None):
+         dry_prob=None, wet_prob=None, wind_bias=None):
     """The fused production step over slots [0, n).  `met` is a dict with
     u0, v0, w0, u1, v1, w1 ((nx, ny, nz) float32) and heights (nz,)."""
     u0 = np.ascontiguousarray(met["u0"], np.float32)
@@ -382,11 +382,13 @@ def step(state: State, n, met, pbl: Pbl, params: StepParams, wet_cells_lf=None, 
     threads = threads or (os.cpu_count() or 1)
     st = state.cstruct()
     pc = pbl.cstruct() if pbl is not None else (_PblF64 if state.dtype == np.float64 else _PblF32)()
-    getattr(lib, "orc_step" + _sfx(state.dtype))(
+    bias = None if wind_bias is None else np.ascontiguousarray(wind_bias, np.float64).reshape(-1)
+    assert bias is None or bias.size == 3 * nx * ny * nz
+    getattr(lib, "orc_step_biased" + _sfx(state.dtype))(
         ctypes.byref(st), ctypes.c_size_t(n), *[_ptr(a) for a in arrs],
         ctypes.c_size_t(nx), ctypes.c_size_t(ny), ctypes.c_size_t(nz), _ptr(hts),
         ctypes.byref(pc), ctypes.byref(prm), _ptr(lam), _ptr(fr),
-        ctypes.c_size_t(wnx), ctypes.c_size_t(wny), ctypes.c_int(threads))
+        ctypes.c_size_t(wnx), ctypes.c_size_t(wny), ctypes.c_int(threads), _ptr(bias))
 
 
 def level_of(z, outheights, dtype=np.float32):

@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     names = set()
-    for hdr in ("fpg.h", "fpg_driver.h"):
+    for hdr in ("fpg.h", "fpg_driver.h", "fpg_adjoint.h"):
         txt = open(os.path.join(ROOT, "include", hdr)).read()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
         names |= set(re.findall(r"\b(fpg_[a-z0-9_]+)\s*\(", txt))
@@ -24,7 +24,7 @@ def test_library_exports_every_declared_symbol():
     assert declared, "no declarations parsed"
     missing = [n for n in sorted(declared) if not hasattr(lib, n)]
     assert not missing, missing
-    assert set(_lib.EXPORTED) | set(_lib.EXPORTED_DRIVER) == declared
+    assert set(_lib.EXPORTED) | set(_lib.EXPORTED_DRIVER) | set(_lib.EXPORTED_ADJOINT) == declared
 
 
 def test_status_strings_and_version():
@@ -56,10 +56,11 @@ def test_record_layouts_match_the_c_header(tmp_path):
         "fpg_step_params": R.StepParams, "fpg_pbl_options": R.PblOptions, "fpg_release": R.Release,
         "fpg_grid_domain": R.GridDomain, "fpg_forward_config": R.ForwardConfig, "fpg_met_bracket": R.MetBracket,
         "fpg_forcing": R.Forcing, "fpg_step_report": R.StepReport, "fpg_batch_scenario": R.BatchScenario,
-        "fpg_batch_tuning": R.BatchTuning,
+        "fpg_batch_tuning": R.BatchTuning, "fpg_receptor": R.Receptor,
+        "fpg_inverse_config": R.InverseConfig,
         "fpg_batch_config": R.BatchConfig,
     }
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fpg_driver.h"', "int main(void) {"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fpg_adjoint.h"', "int main(void) {"]
     for c, py in pairs.items():
         lines.append(f'printf("{c} size %zu\\n", sizeof({c}));')
         for name, _ in py._fields_:
