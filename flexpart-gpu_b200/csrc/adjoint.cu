@@ -11,14 +11,20 @@
 //   turbulence  (z1, tu, tv, tw)  -> (z2, tu', tv', tw')   (Hanna at z1,
 //               Langevin, vertical sub-steps with reflection)
 //   deposition  m -> m * survival                          (survival fixed)
-// The tape kernel re-runs the step with the turbulence block on dual numbers
+// The tape kernel runs the step with the turbulence block on dual numbers
 // (dual.cuh), which gives its 2x2 vertical and per-component horizontal
 // Jacobians with values identical to the plain step, and records the
-// advection points, clamp states, survival and the receptor seeds.  The
-// adjoint kernel then applies the transposed step to the adjoint state
-// lambda, re-gathering the two wind samples' corners for their spatial
-// derivatives and scattering lambda_sample x trilinear weight into the bias
-// gradient.
+// advection points, clamp states, survival and the output state.  The
+// adjoint kernel then adds the receptor term of sampling steps and applies
+// the transposed step to the adjoint state lambda, re-gathering the two wind
+// samples' corners for their spatial derivatives and scattering
+// lambda_sample x trilinear weight into the bias gradient.
+//
+// The tape is recorded either during the forward itself (checkpoint_every
+// == 0: one tape slice per step, no recompute) or, to bound memory, per
+// K-step window from checkpoints during the backward.  Tape slices are
+// indexed on the device by step % slices, so one captured graph serves
+// every step of either mode.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,13 +44,23 @@ enum TapeField {
     T_X0, T_Y0, T_Z0, T_PX, T_PY, T_PZ,          // advection input point and predictor point
     T_ZZ, T_ZTW, T_WZ, T_WTW, T_UZ, T_UU, T_VZ, T_VV,  // turbulence Jacobian
     T_SURV, T_FLAGS,                             // mass survival, clamp bits | TAPE_ACTIVE
-    T_SX, T_SY, T_SZ, T_SM,                      // receptor seeds of the step's output state
+    T_X2, T_Y2, T_Z2, T_M2,                      // the step's output state (receptor term)
     TAPE_FIELDS
 };
 constexpr uint32_t TAPE_ACTIVE = 0x80000000u;
 
 enum LamField { L_X, L_Y, L_Z, L_TU, L_TV, L_TW, L_M, LAM_FIELDS };
 
+// Tape slice j of a step holds TAPE_FIELDS arrays of `cap` floats at
+// base + j * TAPE_FIELDS * cap.
+struct TapeBase {
+    float* base;
+    size_t cap;
+    uint32_t slices;
+    __device__ __forceinline__ float* field(uint32_t j, int f) const {
+        return base + ((size_t)j * TAPE_FIELDS + (size_t)f) * cap;
+    }
+};
 struct TapeArrays { float* f[TAPE_FIELDS]; };
 struct LamArrays { float* f[LAM_FIELDS]; };
 
@@ -119,9 +135,6 @@ __global__ void __launch_bounds__(256) inverse_sample_kernel(const BatchState* s
 struct TapeRec {
     static constexpr bool on = true;
     TapeArrays t;
-    const Receptors* r;
-    uint32_t inst;
-    bool output;
     __device__ __forceinline__ void advect(uint32_t p, float x0, float y0, float z0, float px, float py, float pz,
                                            uint32_t fl) {
         t.f[T_X0][p] = x0; t.f[T_Y0][p] = y0; t.f[T_Z0][p] = z0;
@@ -134,38 +147,32 @@ struct TapeRec {
         t.f[T_UZ][p] = uz; t.f[T_UU][p] = uu; t.f[T_VZ][p] = vz; t.f[T_VV][p] = vv;
     }
     __device__ __forceinline__ void deposit(uint32_t p, float s) { t.f[T_SURV][p] = s; }
-    // dL/d(output state) of the receptor term of this sampling step
     __device__ __forceinline__ void out(uint32_t p, float x, float y, float z, float m) {
-        float sx = 0.0f, sy = 0.0f, sz = 0.0f, sm = 0.0f;
-        if (output) {
-            const Cic c = cic(*r, x, y, z);
-#pragma unroll
-            for (int di = 0; di < 2; ++di)
-#pragma unroll
-                for (int dj = 0; dj < 2; ++dj) {
-                    const int rr = receptor_at(*r, inst, c.i0 + di, c.j0 + dj);
-                    if (rr < 0) continue;
-                    const float g = r->g[rr];
-                    const float wxy = c.wx[di] * c.wy[dj];
-                    sm += g * (wxy * c.v);
-                    sx += g * m * ((di ? 1.0f : -1.0f) * c.wy[dj] * c.v);
-                    sy += g * m * (c.wx[di] * (dj ? 1.0f : -1.0f) * c.v);
-                    sz += g * m * (wxy * c.dv);
-                }
-        }
-        t.f[T_SX][p] = sx; t.f[T_SY][p] = sy; t.f[T_SZ][p] = sz; t.f[T_SM][p] = sm;
+        t.f[T_X2][p] = x; t.f[T_Y2][p] = y; t.f[T_Z2][p] = z; t.f[T_M2][p] = m;
     }
 };
 
-__global__ void __launch_bounds__(256, 2) inverse_tape_kernel(StepArgs a, const BatchState* st,
+// Post-advance clock and scenario state of the step, kept per tape slice.
+__global__ void inverse_snapshot_kernel(const BatchState* st, const ScenDev* __restrict__ sc, uint32_t n_scen,
+                                        uint32_t slices, BatchState* st_all, ScenDev* sc_all) {
+    const uint32_t j = st->step % slices;
+    if (threadIdx.x == 0 && blockIdx.x == 0) st_all[j] = *st;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_scen; s += gridDim.x * blockDim.x)
+        sc_all[(size_t)j * n_scen + s] = sc[s];
+}
+
+__global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const BatchState* st,
                                                               const ScenDev* __restrict__ sc,
                                                               const uint2* __restrict__ items, uint32_t n_items,
-                                                              uint32_t* work, TapeArrays tape, Receptors r) {
+                                                              uint32_t* work, TapeBase tb) {
     extern __shared__ float s_heights[];
     __shared__ uint32_t s_item;
     for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
     const float alpha = st->alpha;
-    const bool output = r.every != 0 && (st->step + 1u) % r.every == 0u;
+    const uint32_t slice = st->step % tb.slices;
+    TapeRec rec;
+#pragma unroll
+    for (int f = 0; f < TAPE_FIELDS; ++f) rec.t.f[f] = tb.field(slice, f);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(work, 1u);
@@ -178,10 +185,9 @@ __global__ void __launch_bounds__(256, 2) inverse_tape_kernel(StepArgs a, const 
         if (local >= d.released) continue;
         const uint32_t p = d.offset + local;
         if (!(a.flags[p] & FLAG_ACTIVE)) {
-            reinterpret_cast<uint32_t*>(tape.f[T_FLAGS])[p] = 0u;
+            reinterpret_cast<uint32_t*>(rec.t.f[T_FLAGS])[p] = 0u;
             continue;
         }
-        TapeRec rec{tape, &r, d.instance, output};
         particle_step_t<TapeRec>(a, s_heights, p, local, alpha, d.counter, d.key0, d.key1, rec);
     }
 }
@@ -216,13 +222,45 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// Sums each of the 24 values v[0..23] over the 32 lanes with a transposed
+// butterfly (12 + 6 + 3 exchanges halve the values a lane holds while
+// doubling the lanes summed, then 2 x 3 exchanges finish the 3 left): 27
+// shuffles instead of 24 x 5.  On return v[0..2] of every lane hold the
+// full sums of values 3c .. 3c+2, c = lane >> 2 (lanes 4c .. 4c+3 agree).
+__device__ __forceinline__ void warp_sum24(float (&v)[24], unsigned lane) {
+    const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        const float send = b4 ? v[i] : v[i + 12];
+        const float keep = b4 ? v[i + 12] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const float send = b3 ? v[i] : v[i + 6];
+        const float keep = b3 ? v[i + 6] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float send = b2 ? v[i] : v[i + 3];
+        const float keep = b2 ? v[i + 3] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        v[i] += __shfl_xor_sync(0xffffffffu, v[i], 2);
+        v[i] += __shfl_xor_sync(0xffffffffu, v[i], 1);
+    }
+}
+
 // Vector-Jacobian product of one dual-time trilinear sample: given lambda of
 // its (u, v, w), returns lambda . d(u, v, w)/d(x, y, z) and adds lambda x
 // corner weight to the bias gradient of each corner node (the bias enters
 // both frames, whose time weights sum to one).  Called by the whole warp;
 // lanes with valid == false contribute nothing.  The bias terms of lanes
-// whose samples share a corner set are summed across the warp first, so one
-// lane per distinct set issues the 24 atomics.
+// whose samples share a corner set are summed across the warp first, and
+// eight lanes then issue one corner's three atomics each.
 __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts, bool valid, float x, float y,
                                              float z, float alpha, float lu, float lv, float lw,
                                              double* __restrict__ dbias) {
@@ -263,21 +301,25 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts
             const uint32_t k0 = __shfl_sync(0xffffffffu, key, src);
             const bool mine = valid && key == k0;
             const unsigned grp = __ballot_sync(0xffffffffu, mine);
+            float v[24];
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j)
-#pragma unroll
-                    for (int k = 0; k < 2; ++k) {
-                        const float c = mine ? wx[i] * wy[j] * wz[k] : 0.0f;
-                        const float su = warp_sum(c * lu), sv = warp_sum(c * lv), sw = warp_sum(c * lw);
-                        if (lane == (unsigned)src && (su != 0.0f || sv != 0.0f || sw != 0.0f)) {
-                            const uint32_t n = (xs[i] * a.ny + ys[j]) * a.nz + zs[k];
-                            atomicAdd(dbias + 3u * n + 0u, (double)su);
-                            atomicAdd(dbias + 3u * n + 1u, (double)sv);
-                            atomicAdd(dbias + 3u * n + 2u, (double)sw);
-                        }
-                    }
+            for (int c = 0; c < 8; ++c) {
+                const float w = mine ? wx[c >> 2] * wy[(c >> 1) & 1] * wz[c & 1] : 0.0f;
+                v[3 * c] = w * lu; v[3 * c + 1] = w * lv; v[3 * c + 2] = w * lw;
+            }
+            warp_sum24(v, lane);
+            // the group's corner set is the source lane's; lane 4c issues corner c
+            const uint32_t cx = __shfl_sync(0xffffffffu, x1, src), cy = __shfl_sync(0xffffffffu, y1, src);
+            const uint32_t cz = __shfl_sync(0xffffffffu, z1, src);
+            if ((lane & 3u) == 0u && (v[0] != 0.0f || v[1] != 0.0f || v[2] != 0.0f)) {
+                const uint32_t c = lane >> 2;
+                const uint32_t bx = k0 / (a.ny * a.nz), by = (k0 / a.nz) % a.ny, bz = k0 % a.nz;
+                const uint32_t n = (((c >> 2) ? cx : bx) * a.ny + (((c >> 1) & 1u) ? cy : by)) * a.nz +
+                                   ((c & 1u) ? cz : bz);
+                atomicAdd(dbias + 3u * n + 0u, (double)v[0]);
+                atomicAdd(dbias + 3u * n + 1u, (double)v[1]);
+                atomicAdd(dbias + 3u * n + 2u, (double)v[2]);
+            }
             pending &= ~grp;
         }
     }
@@ -297,19 +339,45 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts
     return make_float3(gx * ix, gy * iy, gz * iz);
 }
 
-// One work item is 256 slots of one scenario, so a warp's lanes share the
-// scenario: the release gradients are summed across the warp first.
-__global__ void __launch_bounds__(256, 2) inverse_adjoint_kernel(StepArgs a, const BatchState* st,
+// dL/d(output state) of the receptor term of a sampling step.
+__device__ __forceinline__ void receptor_seed(const Receptors& r, uint32_t inst, float x, float y, float z, float m,
+                                              float& sx, float& sy, float& sz, float& sm) {
+    sx = sy = sz = sm = 0.0f;
+    const Cic c = cic(r, x, y, z);
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj) {
+            const int rr = receptor_at(r, inst, c.i0 + di, c.j0 + dj);
+            if (rr < 0) continue;
+            const float g = r.g[rr];
+            const float wxy = c.wx[di] * c.wy[dj];
+            sm += g * (wxy * c.v);
+            sx += g * m * ((di ? 1.0f : -1.0f) * c.wy[dj] * c.v);
+            sy += g * m * (c.wx[di] * (dj ? 1.0f : -1.0f) * c.v);
+            sz += g * m * (wxy * c.dv);
+        }
+}
+
+// The reverse of step `slice`'s tape.  One work item is 256 slots of one
+// scenario, so a warp's lanes share the scenario: the release gradients are
+// summed across the warp first.
+__global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, const BatchState* st,
                                                                  const ScenDev* __restrict__ sc,
                                                                  const uint2* __restrict__ items, uint32_t n_items,
-                                                                 uint32_t* work, TapeArrays tape, LamArrays lam,
+                                                                 uint32_t* work, TapeBase tb, uint32_t slice,
+                                                                 LamArrays lam, Receptors r,
                                                                  double* __restrict__ dbias,
                                                                  double* __restrict__ dsrc) {
     extern __shared__ float s_heights[];
     __shared__ uint32_t s_item;
     for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
     const float alpha = st->alpha;
+    const bool output = r.every != 0 && (st->step + 1u) % r.every == 0u;
     const float kx = a.xs * a.dt, ky = a.ys * a.dt, kz = a.zs * a.dt;
+    TapeArrays tape;
+#pragma unroll
+    for (int f = 0; f < TAPE_FIELDS; ++f) tape.f[f] = tb.field(slice, f);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(work, 1u);
@@ -327,12 +395,17 @@ __global__ void __launch_bounds__(256, 2) inverse_adjoint_kernel(StepArgs a, con
         float zz = 0.0f, ztw = 0.0f, wz = 0.0f, wtw = 0.0f, uz = 0.0f, uu = 0.0f, vz = 0.0f, vv = 0.0f;
         float px = 0.0f, py = 0.0f, pz = 0.0f, x0 = 0.0f, y0 = 0.0f, z0 = 0.0f;
         if (valid) {
-            // adjoint of the step's output state, plus this step's receptor term
-            lx = lam.f[L_X][p] + tape.f[T_SX][p];
-            ly = lam.f[L_Y][p] + tape.f[T_SY][p];
-            lz = lam.f[L_Z][p] + tape.f[T_SZ][p];
+            lx = lam.f[L_X][p]; ly = lam.f[L_Y][p]; lz = lam.f[L_Z][p];
             ltu = lam.f[L_TU][p]; ltv = lam.f[L_TV][p]; ltw = lam.f[L_TW][p];
-            lm = (lam.f[L_M][p] + tape.f[T_SM][p]) * tape.f[T_SURV][p];
+            lm = lam.f[L_M][p];
+            if (output) {
+                // the receptor term of this step's output state
+                float sx, sy, sz, sm;
+                receptor_seed(r, d.instance, tape.f[T_X2][p], tape.f[T_Y2][p], tape.f[T_Z2][p], tape.f[T_M2][p],
+                              sx, sy, sz, sm);
+                lx += sx; ly += sy; lz += sz; lm += sm;
+            }
+            lm = lm * tape.f[T_SURV][p];
             zz = tape.f[T_ZZ][p]; ztw = tape.f[T_ZTW][p]; wz = tape.f[T_WZ][p]; wtw = tape.f[T_WTW][p];
             uz = tape.f[T_UZ][p]; uu = tape.f[T_UU][p]; vz = tape.f[T_VZ][p]; vv = tape.f[T_VV][p];
             px = tape.f[T_PX][p]; py = tape.f[T_PY][p]; pz = tape.f[T_PZ][p];
@@ -417,23 +490,29 @@ struct InverseData {
     float4* ring_raw = nullptr;
     float* bias = nullptr;
     bool has_bias = false;
+    bool tape_in_forward = false;        // checkpoint_every == 0
+    uint32_t slices = 0;                 // tape slices: all steps, or the window length K
     uint32_t n_ckpt = 0;
-    uint32_t* ckpt = nullptr;           // n_ckpt * kNumCkptFields * capacity
+    uint32_t* ckpt = nullptr;            // n_ckpt * kNumCkptFields * capacity
     BatchState* ckpt_st = nullptr;
     ScenDev* ckpt_sc = nullptr;
-    BatchState* win_st = nullptr;       // K post-advance states of the window
-    ScenDev* win_sc = nullptr;
-    float* tape = nullptr;              // K * TAPE_FIELDS * capacity
-    float* lam = nullptr;               // LAM_FIELDS * capacity
+    BatchState* st_all = nullptr;        // post-advance state per tape slice
+    ScenDev* sc_all = nullptr;
+    float* tape = nullptr;               // slices * TAPE_FIELDS * capacity
+    float* lam = nullptr;                // LAM_FIELDS * capacity
     double* dbias = nullptr;
-    float* dbias_f = nullptr;           // float copy for the host
+    float* dbias_f = nullptr;            // float copy for the host
     double* dsrc = nullptr;
-    uint2* items = nullptr;             // 256-slot work items
+    uint2* items = nullptr;              // 256-slot work items
     uint32_t n_items = 0;
     uint32_t* work = nullptr;
     bool forward_done = false;
     uint64_t bytes = 0;
     uint32_t grid_tape = 0, grid_adj = 0;  // persistent grids: SMs x resident CTAs
+    // one taped step (pre, snapshot, tape pass, [sampling], end), captured
+    cudaGraph_t tape_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t tape_exec[2] = {nullptr, nullptr};
+    uint64_t tape_launches[2] = {0, 0};
 
     Receptors receptors_args(uint32_t nx, uint32_t ny) const {
         Receptors r;
@@ -465,18 +544,45 @@ struct fpg_inverse {
     InverseData d;
 };
 
-static TapeArrays tape_arrays(fpg_inverse* v, uint32_t step_in_window) {
-    TapeArrays t;
-    const size_t cap = v->b->capacity;
-    for (int f = 0; f < TAPE_FIELDS; ++f)
-        t.f[f] = v->d.tape + ((size_t)step_in_window * TAPE_FIELDS + f) * cap;
-    return t;
-}
+static TapeBase tape_base(fpg_inverse* v) { return TapeBase{v->d.tape, v->b->capacity, v->d.slices}; }
 
 static LamArrays lam_arrays(fpg_inverse* v) {
     LamArrays l;
     for (int f = 0; f < LAM_FIELDS; ++f) l.f[f] = v->d.lam + (size_t)f * v->b->capacity;
     return l;
+}
+
+// One taped step: the forward step with the tape pass in place of the plain
+// particle pass; `sample` adds the receptor sampling (forward runs).
+static void enqueue_taped_step(fpg_inverse* v, bool sample, cudaStream_t s) {
+    fpg_batch* b = v->b;
+    InverseData& d = v->d;
+    enqueue_pre(b, s);
+    inverse_snapshot_kernel<<<1, 256, 0, s>>>(b->st, b->sc, (uint32_t)b->scen.size(), d.slices, d.st_all, d.sc_all);
+    cudaMemsetAsync(d.work, 0, 4, s);
+    inverse_tape_kernel<<<d.grid_tape, 256, b->met->nz * sizeof(float), s>>>(make_step_args(b), b->st, b->sc,
+                                                                             d.items, d.n_items, d.work,
+                                                                             tape_base(v));
+    b->ctx->count(2);
+    if (sample) enqueue_inverse_sample(b, s);
+    enqueue_end(b, s);
+}
+
+static fpg_status ensure_tape_graph(fpg_inverse* v, int sample) {
+    InverseData& d = v->d;
+    if (d.tape_exec[sample]) return FPG_OK;
+    cudaStream_t s = v->b->ctx->stream;
+    FPG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = v->b->ctx->launches.load();
+    enqueue_taped_step(v, sample != 0, s);
+    d.tape_launches[sample] = v->b->ctx->launches.load() - before;
+    v->b->ctx->launches.fetch_sub(d.tape_launches[sample]);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess) return cuda_status(e);
+    d.tape_graph[sample] = g;
+    FPG_CUDA(cudaGraphInstantiate(&d.tape_exec[sample], g, 0));
+    return FPG_OK;
 }
 
 static fpg_status rebuild_ring(fpg_inverse* v) {
@@ -530,9 +636,14 @@ extern "C" fpg_status fpg_inverse_destroy(fpg_inverse* v) {
         v->b->inv = nullptr;
     }
     InverseData& d = v->d;
+    for (int k = 0; k < 2; ++k) {
+        if (d.tape_exec[k]) cudaGraphExecDestroy(d.tape_exec[k]);
+        if (d.tape_graph[k]) cudaGraphDestroy(d.tape_graph[k]);
+    }
     cudaFree(d.rmap); cudaFree(d.sim); cudaFree(d.g); cudaFree(d.ring_raw); cudaFree(d.bias);
-    cudaFree(d.ckpt); cudaFree(d.ckpt_st); cudaFree(d.ckpt_sc); cudaFree(d.win_st); cudaFree(d.win_sc);
-    cudaFree(d.tape); cudaFree(d.lam); cudaFree(d.dbias); cudaFree(d.dbias_f); cudaFree(d.dsrc); cudaFree(d.items); cudaFree(d.work);
+    cudaFree(d.ckpt); cudaFree(d.ckpt_st); cudaFree(d.ckpt_sc); cudaFree(d.st_all); cudaFree(d.sc_all);
+    cudaFree(d.tape); cudaFree(d.lam); cudaFree(d.dbias); cudaFree(d.dbias_f); cudaFree(d.dsrc);
+    cudaFree(d.items); cudaFree(d.work);
     fpg_batch_destroy(v->b);
     delete v;
     return FPG_OK;
@@ -543,8 +654,7 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
                                          const float* heights, const fpg_receptor* rec, size_t n_rec,
                                          fpg_inverse** out) {
     if (!ctx || !cfg || !src || !out || n_src == 0 || (n_rec && !rec)) return FPG_ERR_INVALID_ARGUMENT;
-    if (cfg->checkpoint_every == 0 || !(cfg->receptor_ramp_m > 0.0f) || !std::isfinite(cfg->receptor_top_m))
-        return FPG_ERR_INVALID_ARGUMENT;
+    if (!(cfg->receptor_ramp_m > 0.0f) || !std::isfinite(cfg->receptor_top_m)) return FPG_ERR_INVALID_ARGUMENT;
     uint32_t n_inst = 1;
     if (src_instance)
         for (size_t s = 0; s < n_src; ++s) n_inst = std::max(n_inst, src_instance[s] + 1u);
@@ -565,8 +675,11 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     for (size_t s = 0; s < n_src; ++s) b->scen[s].instance = src_instance ? src_instance[s] : 0u;
     d.nodes = nx * ny * nz;
     const size_t cells = nx * ny, cap = b->capacity;
-    const uint32_t K = cfg->checkpoint_every;
-    d.n_ckpt = (uint32_t)((b->total_steps + K - 1) / K);
+    d.tape_in_forward = cfg->checkpoint_every == 0;
+    const uint32_t K = d.tape_in_forward ? (uint32_t)b->total_steps
+                                         : (uint32_t)std::min<uint64_t>(cfg->checkpoint_every, b->total_steps);
+    d.slices = K;
+    d.n_ckpt = d.tape_in_forward ? 0u : (uint32_t)((b->total_steps + K - 1) / K);
     // work items of 256 slots for the tape and adjoint kernels
     std::vector<uint2> items;
     for (size_t s = 0; s < n_src; ++s)
@@ -584,10 +697,10 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = alloc((void**)&d.ring_raw, d.nodes * bc.n_frames * sizeof(float4));
     if (e == cudaSuccess) e = alloc((void**)&d.bias, d.nodes * 3 * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.ckpt, (size_t)d.n_ckpt * kNumCkptFields * cap * 4);
-    if (e == cudaSuccess) e = alloc((void**)&d.ckpt_st, d.n_ckpt * sizeof(BatchState));
-    if (e == cudaSuccess) e = alloc((void**)&d.ckpt_sc, (size_t)d.n_ckpt * n_src * sizeof(ScenDev));
-    if (e == cudaSuccess) e = alloc((void**)&d.win_st, K * sizeof(BatchState));
-    if (e == cudaSuccess) e = alloc((void**)&d.win_sc, (size_t)K * n_src * sizeof(ScenDev));
+    if (e == cudaSuccess) e = alloc((void**)&d.ckpt_st, std::max<uint32_t>(d.n_ckpt, 1) * sizeof(BatchState));
+    if (e == cudaSuccess) e = alloc((void**)&d.ckpt_sc, (size_t)std::max<uint32_t>(d.n_ckpt, 1) * n_src * sizeof(ScenDev));
+    if (e == cudaSuccess) e = alloc((void**)&d.st_all, K * sizeof(BatchState));
+    if (e == cudaSuccess) e = alloc((void**)&d.sc_all, (size_t)K * n_src * sizeof(ScenDev));
     if (e == cudaSuccess) e = alloc((void**)&d.tape, (size_t)K * TAPE_FIELDS * cap * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.lam, (size_t)LAM_FIELDS * cap * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.dbias, d.nodes * 3 * 8);
@@ -602,12 +715,9 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = cudaMemsetAsync(d.bias, 0, d.nodes * 3 * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d.ring_raw, 0, d.nodes * bc.n_frames * sizeof(float4), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        fpg_inverse_destroy(v);
-        return cuda_status(e);
-    }
     int per_sm_tape = 0, per_sm_adj = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tape, inverse_tape_kernel, 256, nz * sizeof(float));
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tape, inverse_tape_kernel, 256, nz * sizeof(float));
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adj, inverse_adjoint_kernel, 256, nz * sizeof(float));
     if (e != cudaSuccess) {
@@ -670,12 +780,20 @@ extern "C" fpg_status fpg_inverse_forward(fpg_inverse* v, double* simulated) {
     fpg_status st = batch_reset(b);
     if (st != FPG_OK) return st;
     FPG_CUDA(cudaMemsetAsync(d.sim, 0, std::max<size_t>(d.receptors.size(), 1) * 8, s));
-    if ((st = ensure_graph(b)) != FPG_OK) return st;
-    const uint32_t K = d.cfg.checkpoint_every;
-    for (uint64_t k = 0; k < b->total_steps; ++k) {
-        if (k % K == 0) FPG_CUDA(save_checkpoint(v, (uint32_t)(k / K)));
-        FPG_CUDA(cudaGraphLaunch(b->exec, s));
-        b->ctx->count(b->graph_launches);
+    if (d.tape_in_forward) {
+        if ((st = ensure_tape_graph(v, 1)) != FPG_OK) return st;
+        for (uint64_t k = 0; k < b->total_steps; ++k) {
+            FPG_CUDA(cudaGraphLaunch(d.tape_exec[1], s));
+            b->ctx->count(d.tape_launches[1]);
+        }
+    } else {
+        if ((st = ensure_graph(b)) != FPG_OK) return st;
+        const uint32_t K = d.slices;
+        for (uint64_t k = 0; k < b->total_steps; ++k) {
+            if (k % K == 0) FPG_CUDA(save_checkpoint(v, (uint32_t)(k / K)));
+            FPG_CUDA(cudaGraphLaunch(b->exec, s));
+            b->ctx->count(b->graph_launches);
+        }
     }
     b->steps_done = b->total_steps;
     if (simulated && !d.receptors.empty())
@@ -696,7 +814,6 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
     fpg_batch* b = v->b;
     cudaStream_t s = b->ctx->stream;
     const size_t n_src = b->scen.size(), cap = b->capacity;
-    const uint32_t K = d.cfg.checkpoint_every;
     std::vector<float> g(std::max<size_t>(d.receptors.size(), 1), 0.0f);
     for (size_t r = 0; r < d.receptors.size(); ++r) g[r] = (float)d_sim[r];
     FPG_CUDA(cudaMemcpyAsync(d.g, g.data(), g.size() * 4, cudaMemcpyHostToDevice, s));
@@ -706,35 +823,31 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
     const StepArgs a = make_step_args(b);
     const Receptors rargs = d.receptors_args((uint32_t)b->met->nx, (uint32_t)b->met->ny);
     const LamArrays lam = lam_arrays(v);
+    const TapeBase tb = tape_base(v);
     const size_t smem = b->met->nz * sizeof(float);
-    const uint32_t grid_tape = d.grid_tape, grid_adj = d.grid_adj;
     const uint64_t n = b->total_steps;
-    for (int64_t w = (int64_t)d.n_ckpt - 1; w >= 0; --w) {
+    const uint32_t K = d.slices;
+    const int64_t windows = d.tape_in_forward ? 1 : (int64_t)d.n_ckpt;
+    fpg_status st = FPG_OK;
+    if (!d.tape_in_forward && (st = ensure_tape_graph(v, 0)) != FPG_OK) return st;
+    for (int64_t w = windows - 1; w >= 0; --w) {
         const uint64_t k0 = (uint64_t)w * K, k1 = std::min<uint64_t>(k0 + K, n);
-        FPG_CUDA(restore_checkpoint(v, (uint32_t)w));
-        // taped recompute of the window
-        for (uint64_t k = k0; k < k1; ++k) {
-            const uint32_t j = (uint32_t)(k - k0);
-            enqueue_pre(b, s);
-            FPG_CUDA(cudaMemcpyAsync(d.win_st + j, b->st, sizeof(BatchState), cudaMemcpyDeviceToDevice, s));
-            FPG_CUDA(cudaMemcpyAsync(d.win_sc + (size_t)j * n_src, b->sc, n_src * sizeof(ScenDev),
-                                     cudaMemcpyDeviceToDevice, s));
-            FPG_CUDA(cudaMemsetAsync(d.work, 0, 4, s));
-            inverse_tape_kernel<<<grid_tape, 256, smem, s>>>(a, b->st, b->sc, d.items, d.n_items, d.work,
-                                                             tape_arrays(v, j), rargs);
-            b->ctx->count(1);
-            enqueue_end(b, s);
-            FPG_CHECK_LAUNCH();
+        if (!d.tape_in_forward) {
+            // taped recompute of the window from its checkpoint
+            FPG_CUDA(restore_checkpoint(v, (uint32_t)w));
+            for (uint64_t k = k0; k < k1; ++k) {
+                FPG_CUDA(cudaGraphLaunch(d.tape_exec[0], s));
+                b->ctx->count(d.tape_launches[0]);
+            }
         }
         // reverse of the window
         for (uint64_t k = k1; k-- > k0;) {
-            const uint32_t j = (uint32_t)(k - k0);
-            FPG_CUDA(cudaMemcpyAsync(b->st, d.win_st + j, sizeof(BatchState), cudaMemcpyDeviceToDevice, s));
-            enqueue_pack_forced(b, s);
+            const uint32_t j = (uint32_t)(k % K);
+            enqueue_pack_forced(b, d.st_all + j, s);
             FPG_CUDA(cudaMemsetAsync(d.work, 0, 4, s));
-            inverse_adjoint_kernel<<<grid_adj, 256, smem, s>>>(a, d.win_st + j, d.win_sc + (size_t)j * n_src,
-                                                               d.items, d.n_items, d.work, tape_arrays(v, j), lam,
-                                                               d_bias ? d.dbias : nullptr, d.dsrc);
+            inverse_adjoint_kernel<<<d.grid_adj, 256, smem, s>>>(a, d.st_all + j, d.sc_all + (size_t)j * n_src,
+                                                                 d.items, d.n_items, d.work, tb, j, lam, rargs,
+                                                                 d_bias ? d.dbias : nullptr, d.dsrc);
             b->ctx->count(1);
             FPG_CHECK_LAUNCH();
         }
@@ -756,9 +869,9 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
             d_pos[3 * k + 2] = src[4 * k + 2];
         }
     }
-    // the population now holds the first window's recompute: the forward
-    // must run again before the next backward
-    d.forward_done = false;
+    // with checkpoints the population now holds the first window's
+    // recompute; the tape of a taped forward stays valid for another backward
+    if (!d.tape_in_forward) d.forward_done = false;
     return FPG_OK;
 }
 

@@ -408,9 +408,9 @@ __global__ void __launch_bounds__(256) batch_pack_forced_kernel(const BatchState
     }
 }
 
-void enqueue_pack_forced(fpg_batch* b, cudaStream_t s) {
+void enqueue_pack_forced(fpg_batch* b, const BatchState* st, cudaStream_t s) {
     const uint32_t nodes = (uint32_t)(b->met->nx * b->met->ny * b->met->nz);
-    batch_pack_forced_kernel<<<b->ctx->sm_count * 4, 256, 0, s>>>(b->st, b->ring, nodes, b->met->bracket);
+    batch_pack_forced_kernel<<<b->ctx->sm_count * 4, 256, 0, s>>>(st, b->ring, nodes, b->met->bracket);
     b->ctx->count(1);
 }
 

@@ -134,8 +134,8 @@ PopFields pop_fields(fpg_batch* b);
 void enqueue_pre(fpg_batch* b, cudaStream_t s);
 void enqueue_step_kernel(fpg_batch* b, cudaStream_t s);
 void enqueue_post(fpg_batch* b, cudaStream_t s);
-// Repacks the bracket of the state's current frames whether or not it changed.
-void enqueue_pack_forced(fpg_batch* b, cudaStream_t s);
+// Repacks the bracket of state st's frames whether or not it changed.
+void enqueue_pack_forced(fpg_batch* b, const BatchState* st, cudaStream_t s);
 fpg_status build_items(fpg_batch* b, uint32_t variant);
 // The counter and clock advance alone (batch_end_kernel).
 void enqueue_end(fpg_batch* b, cudaStream_t s);

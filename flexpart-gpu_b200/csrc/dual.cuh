@@ -6,6 +6,10 @@
 // reproduces the float results bit for bit while the tangents give the
 // local Jacobian.
 //
+// Only the value needs the plain code's rounding: the tangents use the fast
+// reciprocal-based division (__fdividef, within 2 ulp), which is far cheaper
+// than an IEEE division and accurate well beyond what a derivative needs.
+//
 // Derivatives at kinks (the subgradient chosen):
 //   xmax(x, c)        derivative of x when x > c, else 0
 //   xclamp(x, lo, hi) derivative of x when lo < x < hi, else 0
@@ -41,12 +45,17 @@ __device__ __forceinline__ D2 operator*(const D2& x, float c) { return D2(x.v * 
 __device__ __forceinline__ D2 operator*(float c, const D2& x) { return D2(c * x.v, c * x.a, c * x.b); }
 __device__ __forceinline__ D2 operator/(const D2& x, const D2& y) {
     const float q = x.v / y.v;
-    return D2(q, (x.a - q * y.a) / y.v, (x.b - q * y.b) / y.v);
+    const float r = __fdividef(1.0f, y.v);
+    return D2(q, (x.a - q * y.a) * r, (x.b - q * y.b) * r);
 }
-__device__ __forceinline__ D2 operator/(const D2& x, float c) { return D2(x.v / c, x.a / c, x.b / c); }
+__device__ __forceinline__ D2 operator/(const D2& x, float c) {
+    const float r = __fdividef(1.0f, c);
+    return D2(x.v / c, x.a * r, x.b * r);
+}
 __device__ __forceinline__ D2 operator/(float c, const D2& y) {
     const float q = c / y.v;
-    return D2(q, -q * y.a / y.v, -q * y.b / y.v);
+    const float r = -q * __fdividef(1.0f, y.v);
+    return D2(q, r * y.a, r * y.b);
 }
 
 __device__ __forceinline__ D2 xexp(const D2& x) {
@@ -55,17 +64,17 @@ __device__ __forceinline__ D2 xexp(const D2& x) {
 }
 __device__ __forceinline__ D2 xsqrt(const D2& x) {
     const float s = sqrtf(x.v);
-    const float k = 0.5f / s;
+    const float k = __fdividef(0.5f, s);
     return D2(s, x.a == 0.0f ? 0.0f : x.a * k, x.b == 0.0f ? 0.0f : x.b * k);
 }
 __device__ __forceinline__ D2 xcbrt(const D2& x) {
     const float c = cbrtf(x.v);
-    const float k = 1.0f / (3.0f * c * c);
+    const float k = __fdividef(1.0f, 3.0f * c * c);
     return D2(c, x.a == 0.0f ? 0.0f : x.a * k, x.b == 0.0f ? 0.0f : x.b * k);
 }
 __device__ __forceinline__ D2 xpow(const D2& x, float e) {
     const float p = powf(x.v, e);
-    const float k = e * p / x.v;
+    const float k = __fdividef(e * p, x.v);
     return D2(p, x.a == 0.0f ? 0.0f : x.a * k, x.b == 0.0f ? 0.0f : x.b * k);
 }
 __device__ __forceinline__ D2 xmax(const D2& x, float c) {

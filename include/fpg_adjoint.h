@@ -17,7 +17,8 @@
  *   (tent functions of width one cell centred on the cell centre, in grid
  *   coordinates) times a vertical weight that is 1 below
  *   receptor_top_m - ramp/2, 0 above receptor_top_m + ramp/2 and linear
- *   between.  Particle state is checkpointed every K steps.
+ *   between.  Particle state is checkpointed every K steps, or the tape of
+ *   every step is recorded during the forward itself (K = 0).
  * backward: given dL/dsim_r, returns dL/d(source mass), dL/d(source
  *   position: lon, lat, z of the release box, moved rigidly) and dL/d(wind
  *   bias) for a bias field b added to u, v, w at every met node of every
@@ -54,7 +55,11 @@ typedef struct fpg_inverse_config {
     uint32_t sample_every_steps;     /* receptors sampled after steps k with (k + 1) % every == 0 */
     float receptor_top_m;            /* top of the observed layer (100 m) */
     float receptor_ramp_m;           /* width of the vertical weight's linear ramp (> 0) */
-    uint32_t checkpoint_every;       /* K >= 1: particle state saved every K steps */
+    uint32_t checkpoint_every;       /* K >= 1: particle state saved every K steps and each K-step
+                                        window recomputed with its tape in the backward (memory:
+                                        steps/K checkpoints of 44 B per slot + K x 80 B per slot);
+                                        0: the forward records the tape of every step (no recompute;
+                                        steps x 80 B per slot) */
 } fpg_inverse_config;
 
 typedef struct fpg_inverse fpg_inverse;
@@ -80,7 +85,8 @@ fpg_status fpg_inverse_set_sources(fpg_inverse* inv, const double* mass_kg, cons
 fpg_status fpg_inverse_set_wind_bias(fpg_inverse* inv, const float* bias);
 /* Runs the whole forward run and writes sim_r (n_receptors doubles). */
 fpg_status fpg_inverse_forward(fpg_inverse* inv, double* simulated);
-/* After fpg_inverse_forward with the same parameters: the gradient of a
+/* After fpg_inverse_forward with the same parameters (and, with K >= 1, once
+ * per forward: the recompute consumes the checkpointed state): the gradient of a
  * loss L given dL/dsim_r.  d_mass (n_sources), d_position (n_sources * 3:
  * d/dlon [per degree], d/dlat, d/dz [per metre]) and d_wind_bias (nodes*3)
  * may each be NULL. */

@@ -2,7 +2,8 @@
 
 * The inversion's forward is the batched production step: its particles are
   bit-identical to a plain batch run of the same sources.
-* The gradient does not depend on the checkpoint interval K.
+* The gradient does not depend on the checkpoint interval K, nor on
+  recording the tape in the forward (K = 0) instead of recomputing it.
 * Gradients against central finite differences of the device forward
   (FP32, fixed Philox counters): mass exactly (the loss is quadratic in the
   masses), positions and wind bias on a short horizon with steps where the
@@ -76,7 +77,7 @@ def test_inversion_forward_is_the_batched_step(ctx):
 
 def test_gradient_does_not_depend_on_the_checkpoint_interval(ctx):
     grads = []
-    for K in (1, 4, 1000):
+    for K in (0, 1, 4, 1000):
         inv = _problem(3, smooth=False, K=K)
         model = adj.SourceInversion(ctx, inv)
         sim = model.forward(model.mass0, model.position0)
