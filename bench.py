@@ -25,6 +25,9 @@ concentration grid is read back every step.
 The line's "batched" object is the batched ensemble (run_batched): 256
 release scenarios stepped as one population, one CUDA-graph replay per step,
 against interleaved plain launches and scenario-by-scenario driver runs.
+Its "adjoint" object is the source inversion's forward + backward
+(run_adjoint): the 16-source, 1 M-particle inversion and the 64-instance
+batched inversion with checkpoints every 8 steps.
 
 Under torchrun each rank runs its own 10 M-particle shard (weak scaling, met
 replicated, no exchange in the timed region).  Rank 0 prints one JSON line.
@@ -69,6 +72,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-scenarios", type=int, default=256)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-instances", type=int, default=64)
     ap.add_argument("--quick", action="store_true",
                     help="profiling case: no spin-up (particles scattered around the sources), no e2e, no CPU leg")
     return ap.parse_args()
@@ -365,6 +370,102 @@ def run_batched(ctx, stream, args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+def run_adjoint(ctx, stream, args, rank, world):
+    """Forward + adjoint of the source inversion (include/fpg_adjoint.h).
+
+    C3: 1 M particles from 16 sources on the 90x60x20 met, 200 receptors in
+    the lowest layer, 24 h; loss sum (sim - obs)^2 with obs from emissions x
+    lognormal(0, 0.5) plus 10 % noise; gradient w.r.t. 16 masses, 16x3
+    positions and the 90x60x20x3 wind bias.  Timed: the plain forward (no
+    tape), then forward + backward with the tape recorded in the forward
+    (K = 0) and with checkpoints every 8 steps (K = 8).
+    C4: 64 instances (log-uniform [50 k, 2 M] particles, 8 sources and 100
+    receptors each) on the 180x90x40 met, 72 h, checkpoints every 8 steps."""
+    import torch
+    import torch.distributed as dist
+
+    from flexpart_gpu import batch as bt
+    from flexpart_gpu import synthetic
+    from flexpart_gpu.adjoint import SourceInversion, misfit, synthetic_observations
+
+    def timed(fn):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        ctx.synchronize()
+        ms = a.elapsed_time(b)
+        if world > 1:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms, r
+
+    out = {}
+    inv = synthetic.config3(seed=3 + rank)
+    ps = bt.particle_steps(inv.ensemble)
+    res = {}
+    obs = None
+    for K in (8, 0):
+        inv.checkpoint_every = K
+        model = SourceInversion(ctx, inv)
+        if obs is None:
+            obs, _ = synthetic_observations(model)
+        model.forward(model.mass0, model.position0)          # warm-up
+        tf, sim = timed(lambda: model.forward(model.mass0, model.position0))
+        loss, dsim = misfit(sim, obs)
+        tb, g = timed(lambda: model.backward(dsim))
+        res[K] = {"forward_ms": tf, "backward_ms": tb, "device_bytes": model.device_bytes}
+        if K == 0:
+            # spot check: the mass gradient of source 0 against central differences (h = 1e-3 relative)
+            m0 = model.mass0.copy()
+            h = 1e-3 * m0[0]
+            mp, mm = m0.copy(), m0.copy()
+            mp[0] += h
+            mm[0] -= h
+            fd = (misfit(model.forward(mp), obs)[0] - misfit(model.forward(mm), obs)[0]) / (2 * h)
+            out["c3_fd_mass_source0"] = {"adjoint": float(g["mass"][0]), "fd": float(fd),
+                                         "rel_err": abs(float(g["mass"][0]) - fd) / max(abs(fd), 1e-300)}
+        del model
+    plain = res[8]["forward_ms"]
+    out["c3"] = {
+        "workload": "1M particles, 16 sources, 200 receptors, met 90x60x20, 24 h (97 steps)",
+        "particle_steps": ps, "plain_forward_ms": plain, "plain_forward_value": ps * world / (plain / 1e3),
+        "tape_in_forward": {"forward_ms": res[0]["forward_ms"], "backward_ms": res[0]["backward_ms"],
+                            "ratio_to_forward": (res[0]["forward_ms"] + res[0]["backward_ms"]) / plain,
+                            "value": ps * world / ((res[0]["forward_ms"] + res[0]["backward_ms"]) / 1e3),
+                            "device_bytes": res[0]["device_bytes"]},
+        "checkpoint_every_8": {"forward_ms": res[8]["forward_ms"], "backward_ms": res[8]["backward_ms"],
+                               "ratio_to_forward": (res[8]["forward_ms"] + res[8]["backward_ms"]) / plain,
+                               "value": ps * world / ((res[8]["forward_ms"] + res[8]["backward_ms"]) / 1e3),
+                               "device_bytes": res[8]["device_bytes"]},
+    }
+    if args.adjoint_instances > 0:
+        inv4 = synthetic.config4(n_instances=args.adjoint_instances, seed=4 + rank)
+        ps4 = bt.particle_steps(inv4.ensemble)
+        model = SourceInversion(ctx, inv4)
+        rng = np.random.default_rng(11)
+        tf, sim = timed(lambda: model.forward(model.mass0, model.position0))
+        obs4 = sim * (1.0 + 0.1 * rng.standard_normal(sim.size))
+        loss, dsim = misfit(sim, obs4)
+        tb, g = timed(lambda: model.backward(dsim))
+        out["c4"] = {
+            "workload": f"{args.adjoint_instances} inversion instances, {inv4.ensemble.total_particles} particles, "
+                        f"{len(inv4.ensemble.sources)} sources, {len(inv4.receptors)} receptors, met 180x90x40, "
+                        f"72 h ({inv4.ensemble.n_steps} steps), checkpoints every 8 steps",
+            "particle_steps": ps4, "forward_ms": tf, "backward_ms": tb, "ratio_to_forward": (tf + tb) / tf,
+            "value": ps4 * world / ((tf + tb) / 1e3), "device_bytes": model.device_bytes,
+        }
+        del model
+    return out
+
+
+# ---------------------------------------------------------------------------
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -570,6 +671,9 @@ def main():
     batched = None
     if not args.no_batched and not args.quick:
         batched = run_batched(ctx, stream, args, rank, world)
+    adjoint = None
+    if not args.no_adjoint and not args.quick:
+        adjoint = run_adjoint(ctx, stream, args, rank, world)
 
     if rank == 0:
         line = {
@@ -593,6 +697,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     del drv

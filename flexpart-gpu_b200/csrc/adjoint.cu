@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(256) inverse_sample_kernel(const BatchState* s
 struct TapeRec {
     static constexpr bool on = true;
     TapeArrays t;
+    bool output;   // a sampling step: the output state is read by the reverse
     __device__ __forceinline__ void advect(uint32_t p, float x0, float y0, float z0, float px, float py, float pz,
                                            uint32_t fl) {
         t.f[T_X0][p] = x0; t.f[T_Y0][p] = y0; t.f[T_Z0][p] = z0;
@@ -148,7 +149,7 @@ struct TapeRec {
     }
     __device__ __forceinline__ void deposit(uint32_t p, float s) { t.f[T_SURV][p] = s; }
     __device__ __forceinline__ void out(uint32_t p, float x, float y, float z, float m) {
-        t.f[T_X2][p] = x; t.f[T_Y2][p] = y; t.f[T_Z2][p] = z; t.f[T_M2][p] = m;
+        if (output) { t.f[T_X2][p] = x; t.f[T_Y2][p] = y; t.f[T_Z2][p] = z; t.f[T_M2][p] = m; }
     }
 };
 
@@ -164,13 +165,14 @@ __global__ void inverse_snapshot_kernel(const BatchState* st, const ScenDev* __r
 __global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const BatchState* st,
                                                               const ScenDev* __restrict__ sc,
                                                               const uint2* __restrict__ items, uint32_t n_items,
-                                                              uint32_t* work, TapeBase tb) {
+                                                              uint32_t* work, TapeBase tb, uint32_t every) {
     extern __shared__ float s_heights[];
     __shared__ uint32_t s_item;
     for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
     const float alpha = st->alpha;
     const uint32_t slice = st->step % tb.slices;
     TapeRec rec;
+    rec.output = every != 0 && (st->step + 1u) % every == 0u;
 #pragma unroll
     for (int f = 0; f < TAPE_FIELDS; ++f) rec.t.f[f] = tb.field(slice, f);
     for (;;) {
@@ -562,7 +564,7 @@ static void enqueue_taped_step(fpg_inverse* v, bool sample, cudaStream_t s) {
     cudaMemsetAsync(d.work, 0, 4, s);
     inverse_tape_kernel<<<d.grid_tape, 256, b->met->nz * sizeof(float), s>>>(make_step_args(b), b->st, b->sc,
                                                                              d.items, d.n_items, d.work,
-                                                                             tape_base(v));
+                                                                             tape_base(v), d.cfg.sample_every_steps);
     b->ctx->count(2);
     if (sample) enqueue_inverse_sample(b, s);
     enqueue_end(b, s);

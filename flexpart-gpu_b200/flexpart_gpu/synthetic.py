@@ -360,3 +360,44 @@ def make_frames_uniform_pbl(spec: MetSpec):
     for f in frames:
         f["surface"][:] = f["surface"][0]
     return frames
+
+
+def config4(n_instances: int = 64, lo: int = 50_000, hi: int = 2_000_000, hours: int = 72, sources_per: int = 8,
+            receptors_per: int = 100, met: MetSpec | None = None, seed: int = 4) -> Inversion:
+    """n_instances independent source inversions in one batch: particle
+    counts per instance log-uniform in [lo, hi] (about 34 M for 64 in
+    [50 k, 2 M]), split over sources_per point sources (heights U(10, 300)
+    m, 6 h releases from a step in the first half, own Philox keys), and
+    receptors_per distinct receptor cells per instance; met 180x90 (2 deg) x
+    40 levels, 9 frames 3 h apart, wet scavenging on; 72 h (289 steps) at
+    dt 900 s; checkpoints every 8 steps."""
+    if met is None:
+        met = MetSpec(nx=180, ny=90, nz=40, dx_deg=2.0, dy_deg=2.0, xlon0=-179.0, ylat0=-89.0, n_frames=9,
+                      seed=2, wet=True)
+    rng = np.random.default_rng(400 + seed)
+    t0 = EPOCH_2024
+    dt = 900
+    end = t0 + hours * 3600
+    half_steps = max((end - t0) // dt // 2, 1)
+    lon_span = (met.nx - 1) * met.dx_deg
+    lat_span = (met.ny - 1) * met.dy_deg
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), n_instances)).astype(np.int64)
+    sources, keys, instance, receptors = [], [], [], []
+    for n in range(n_instances):
+        per = int(counts[n]) // sources_per
+        for s in range(sources_per):
+            lon = float(met.xlon0 + rng.uniform(0.1, 0.9) * lon_span)
+            lat = float(met.ylat0 + rng.uniform(0.2, 0.8) * lat_span)
+            z = float(rng.uniform(10.0, 300.0))
+            start = int(t0 + dt * int(rng.integers(0, half_steps)))
+            sources.append(Source(lon=lon, lat=lat, z_min=z, z_max=z, mass_kg=1.0, particle_count=max(per, 1),
+                                  start=start, end=min(start + 6 * 3600, end)))
+            keys.append((int(rng.integers(0, 2**32)), 100_000 + n * sources_per + s))
+            instance.append(n)
+        cells = rng.choice(met.nx * met.ny, size=receptors_per, replace=False)
+        receptors += [(n, int(c // met.ny), int(c % met.ny)) for c in cells]
+    ens = Ensemble("config4", met, sources, keys, start=t0, end=end, dt=dt, out_shape=(met.nx, met.ny, 1),
+                   outheights=[100.0])
+    inv = Inversion("config4", ens, receptors, instance, checkpoint_every=8)
+    inv.smooth = False
+    return inv
