@@ -30,7 +30,9 @@ Its "adjoint" object is the source inversion's forward + backward
 batched inversion with checkpoints every 8 steps.
 
 Under torchrun each rank runs its own 10 M-particle shard (weak scaling, met
-replicated, no exchange in the timed region).  Rank 0 prints one JSON line.
+replicated, own Philox stream); the one exchange, at each output time inside
+the timed region, is the NCCL sum of the ranks' integer grids.  Rank 0
+prints one JSON line.
 """
 from __future__ import annotations
 
@@ -486,6 +488,7 @@ def main():
         dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120))
 
     from flexpart_gpu import api, synthetic
+    from flexpart_gpu import distributed as fd
     from flexpart_gpu import timeloop as tl
     from flexpart_gpu.records import StepParams
 
@@ -505,7 +508,7 @@ def main():
     # ---- spin-up through the C-ABI time loop: 48 h of release ----
     t_spin = time.perf_counter()
     cfg = tl.scenario_config(scn, sort_interval_steps=SORT_EVERY,
-                             initial_philox_counter=(rank * 0x10000000, 0, 0, rank))
+                             initial_philox_counter=fd.rank_counter((0, 0, 0, 0), rank))
     drv = tl.ForwardDriver(ctx, cfg, tl.scenario_releases(scn), tl.scenario_domain(scn), args.particles,
                            (spec.nx, spec.ny, spec.nz), heights)
     src = tl.BracketSource(scn, frames)
@@ -548,6 +551,9 @@ def main():
         wet.from_precipitation(precip[fa], None, None, scn.wet_a, scn.wet_b)
 
     ev = []
+    n_out_cells = scn.out_shape[0] * scn.out_shape[1] * scn.out_shape[2]
+    # torch's collectives run on its current stream: make that the library's stream
+    torch.cuda.set_stream(stream)
 
     def one_step(record: bool):
         t = state["t"]
@@ -573,6 +579,10 @@ def main():
             ev.append((a, b))
         if state["k"] % 12 == 11:
             grid.accumulate(parts, 0, 1e6, scn.outheights)
+            if world > 1:
+                # the one exchange: the ranks' integer grids summed (mod 2^32) over NCCL
+                fd.allreduce_grids_device(lib.fpg_grid_counts_device(grid.h), lib.fpg_grid_mass_device(grid.h),
+                                          n_out_cells)
         state["t"] = t + scn.dt
         state["k"] += 1
 
