@@ -101,6 +101,10 @@ extern "C" const char* fpg_status_string(fpg_status s) {
         case FPG_ERR_OUT_OF_GRID: return "release outside grid domain";
         case FPG_ERR_TOO_MANY_LEVELS: return "too many vertical levels";
         case FPG_ERR_INVALID_TIME_RANGE: return "start time after end time";
+        case FPG_ERR_INVALID_BACKWARD_TIME_RANGE: return "backward run: start time before end time";
+        case FPG_ERR_MISSING_RECEPTORS: return "backward run needs at least one receptor";
+        case FPG_ERR_INVALID_RECEPTOR: return "invalid receptor";
+        case FPG_ERR_INVALID_SOURCE_BOUNDS: return "invalid source region bounds";
         case FPG_ERR_CUDA: return "CUDA error";
         case FPG_ERR_OUT_OF_MEMORY: return "out of device memory";
         case FPG_ERR_NO_DEVICE: return "no CUDA device";

@@ -92,6 +92,9 @@ struct fpg_forward {
     int64_t bracket_t0 = 0, bracket_t1 = 0;
     float* d_forcing[3] = {nullptr, nullptr, nullptr};   // dry velocity, wet lambda, wet fraction per slot
     std::vector<fpg_particle> staging;
+    // +1 forward; -1 backward (BackwardTimeLoopDriver): the clock runs back,
+    // advection takes -dt and turbulence/deposition +dt (timeloop.rs:1724-1746)
+    int direction = 1;
 };
 
 using namespace fpg;
@@ -144,12 +147,22 @@ extern "C" fpg_status fpg_forward_destroy(fpg_forward* d) {
     return FPG_OK;
 }
 
+static fpg_status driver_create(fpg_ctx* ctx, const fpg_forward_config* cfg, const fpg_release* rel, size_t n_rel,
+                                const fpg_grid_domain* grid, size_t capacity, size_t nx, size_t ny, size_t nz,
+                                const float* heights, int direction, fpg_forward** out);
+
 extern "C" fpg_status fpg_forward_create(fpg_ctx* ctx, const fpg_forward_config* cfg, const fpg_release* rel,
                                          size_t n_rel, const fpg_grid_domain* grid, size_t capacity, size_t nx,
                                          size_t ny, size_t nz, const float* heights, fpg_forward** out) {
     if (!ctx || !cfg || !grid || !out || (n_rel && !rel)) return FPG_ERR_INVALID_ARGUMENT;
     // validate_config (timeloop.rs:1932-1972)
     if (cfg->start_seconds > cfg->end_seconds) return FPG_ERR_INVALID_TIME_RANGE;
+    return driver_create(ctx, cfg, rel, n_rel, grid, capacity, nx, ny, nz, heights, 1, out);
+}
+
+static fpg_status driver_create(fpg_ctx* ctx, const fpg_forward_config* cfg, const fpg_release* rel, size_t n_rel,
+                                const fpg_grid_domain* grid, size_t capacity, size_t nx, size_t ny, size_t nz,
+                                const float* heights, int direction, fpg_forward** out) {
     if (cfg->timestep_seconds <= 0) return FPG_ERR_INVALID_TIME_STEP;
     if (!std::isfinite(cfg->dry_reference_height_m) || cfg->dry_reference_height_m <= 0.0f)
         return FPG_ERR_INVALID_REFERENCE_HEIGHT;
@@ -160,6 +173,7 @@ extern "C" fpg_status fpg_forward_create(fpg_ctx* ctx, const fpg_forward_config*
     fpg_forward* d = new fpg_forward();
     d->ctx = ctx;
     d->cfg = *cfg;
+    d->direction = direction;
     d->domain = *grid;
     d->capacity = capacity;
     d->t = cfg->start_seconds;
@@ -185,7 +199,10 @@ extern "C" fpg_status fpg_forward_create(fpg_ctx* ctx, const fpg_forward_config*
     return FPG_OK;
 }
 
-extern "C" int32_t fpg_forward_has_remaining_steps(const fpg_forward* d) { return d && d->t <= d->cfg.end_seconds; }
+extern "C" int32_t fpg_forward_has_remaining_steps(const fpg_forward* d) {
+    if (!d) return 0;
+    return d->direction > 0 ? d->t <= d->cfg.end_seconds : d->t >= d->cfg.end_seconds;
+}
 extern "C" int64_t fpg_forward_current_time(const fpg_forward* d) { return d ? d->t : 0; }
 extern "C" fpg_particles* fpg_forward_particles(fpg_forward* d) { return d ? d->particles : nullptr; }
 
@@ -298,7 +315,7 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
     fpg_step_params p;
     fpg_step_params_default(&p);
     p.alpha = alpha;
-    p.dt_seconds = dt;
+    p.dt_seconds = d->direction > 0 ? dt : -dt;   // TimeDirection::advection_dt_seconds (timeloop.rs:137-142)
     p.turb_dt_seconds = dt;
     p.x_grid_per_meter = d->cfg.x_grid_per_meter;
     p.y_grid_per_meter = d->cfg.y_grid_per_meter;
@@ -378,7 +395,7 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
         std::memcpy(report->next_philox_counter, d->counter, sizeof(d->counter));
     }
     d->step_index += 1;
-    d->t += d->cfg.timestep_seconds;
+    d->t += d->direction > 0 ? d->cfg.timestep_seconds : -d->cfg.timestep_seconds;
     return FPG_OK;
 }
 
@@ -390,4 +407,222 @@ extern "C" fpg_status fpg_forward_accumulate_grid(fpg_forward* d, fpg_grid* grid
     const fpg_status st = fpg_grid_accumulate(d->ctx, d->particles, grid, species, scale, outheights, n_oh, nullptr);
     d->particles->dispatch = keep;
     return st;
+}
+
+// ============================================================================
+// Backward (receptor) mode: BackwardTimeLoopDriver (timeloop.rs:1433-1909)
+// ============================================================================
+
+namespace fpg {
+namespace {
+
+struct RegionBox { double lon_min, lon_max, lat_min, lat_max, z_min, z_max; };
+
+// collect_source_collections (timeloop.rs:1865-1894) in one pass: a particle
+// is a hit of a region when its lon = xlon0 + (cell_x + pos_x) * dx, lat
+// likewise and z lie inside the inclusive bounds (contains_particle,
+// :187-197, in double).  Counts are warp-aggregated integer sums; masses are
+// summed in double.  The loop runs in whole warps so every lane reaches the
+// warp votes.
+__global__ void __launch_bounds__(256) region_collect_kernel(const int32_t* __restrict__ cell_x,
+                                                             const int32_t* __restrict__ cell_y,
+                                                             const float* __restrict__ pos_x,
+                                                             const float* __restrict__ pos_y,
+                                                             const float* __restrict__ pos_z,
+                                                             const uint32_t* __restrict__ flags,
+                                                             const float* __restrict__ mass0, uint32_t n,
+                                                             const RegionBox* __restrict__ regions,
+                                                             uint32_t n_regions, fpg_grid_domain g,
+                                                             unsigned long long* __restrict__ hits,
+                                                             double* __restrict__ mass) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t p = base + threadIdx.x;
+        const bool active = p < n && (flags[p] & 1u);
+        double lon = 0.0, lat = 0.0, z = 0.0, m = 0.0;
+        if (active) {
+            lon = g.xlon0 + ((double)cell_x[p] + (double)pos_x[p]) * g.dx;
+            lat = g.ylat0 + ((double)cell_y[p] + (double)pos_y[p]) * g.dy;
+            z = (double)pos_z[p];
+            m = (double)mass0[p];
+        }
+        for (uint32_t r = 0; r < n_regions; ++r) {
+            const RegionBox b = regions[r];
+            const bool in = active && lon >= b.lon_min && lon <= b.lon_max && lat >= b.lat_min &&
+                            lat <= b.lat_max && z >= b.z_min && z <= b.z_max;
+            const unsigned vote = __ballot_sync(0xffffffffu, in);
+            if (vote == 0u) continue;
+            double ms = in ? m : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ms += __shfl_xor_sync(0xffffffffu, ms, o);
+            if (lane == 0u) {
+                atomicAdd(hits + r, (unsigned long long)__popc(vote));
+                atomicAdd(mass + r, ms);
+            }
+        }
+    }
+}
+
+}  // namespace
+}  // namespace fpg
+
+struct fpg_backward {
+    fpg_forward* f = nullptr;
+    std::vector<RegionBox> regions;
+    RegionBox* d_regions = nullptr;
+    unsigned long long* d_hits = nullptr;
+    double* d_mass = nullptr;
+};
+
+extern "C" void fpg_backward_config_default(fpg_backward_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->start_seconds = 1704067200;   // 20240101000000
+    c->end_seconds = 1704067200;
+    c->timestep_seconds = 1;
+    c->clamp_time_bounds = 1;
+    c->x_grid_per_meter = c->y_grid_per_meter = c->z_grid_per_meter = 1.0f;
+    c->pbl_options = fpg_pbl_options{0.1f, 10.0f, 1.0f, 800.0f, 100.0f, 4500.0f};
+    c->dry_reference_height_m = 15.0f;
+    c->philox_key[0] = 0xDECAFBADu;
+    c->philox_key[1] = 0x12345678u;
+    c->n_substeps = 4;
+    c->min_height_m = 0.01f;
+}
+
+extern "C" fpg_status fpg_backward_destroy(fpg_backward* b) {
+    if (!b) return FPG_OK;
+    fpg_forward_destroy(b->f);
+    cudaFree(b->d_regions);
+    cudaFree(b->d_hits);
+    cudaFree(b->d_mass);
+    delete b;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_backward_create(fpg_ctx* ctx, const fpg_backward_config* cfg,
+                                          const fpg_receptor_release* rec, size_t n_rec,
+                                          const fpg_source_region* reg, size_t n_reg, const fpg_grid_domain* grid,
+                                          size_t capacity, size_t nx, size_t ny, size_t nz, const float* heights,
+                                          fpg_backward** out) {
+    if (!ctx || !cfg || !grid || !out || (n_rec && !rec) || (n_reg && !reg)) return FPG_ERR_INVALID_ARGUMENT;
+    // validate_backward_config (timeloop.rs:1974-2003), validate_receptor
+    // (:2006-2046), validate_source_region (:2049-2073)
+    if (cfg->start_seconds < cfg->end_seconds) return FPG_ERR_INVALID_BACKWARD_TIME_RANGE;
+    if (cfg->timestep_seconds <= 0) return FPG_ERR_INVALID_TIME_STEP;
+    if (!std::isfinite(cfg->dry_reference_height_m) || cfg->dry_reference_height_m <= 0.0f)
+        return FPG_ERR_INVALID_REFERENCE_HEIGHT;
+    if (n_rec == 0) return FPG_ERR_MISSING_RECEPTORS;
+    for (size_t i = 0; i < n_rec; ++i) {
+        const fpg_receptor_release& r = rec[i];
+        if (!(r.lon >= -180.0 && r.lon <= 180.0) || !(r.lat >= -90.0 && r.lat <= 90.0) ||
+            !std::isfinite(r.z_m) || r.z_m < 0.0 || r.particle_count == 0 || !std::isfinite(r.mass_kg) ||
+            r.mass_kg <= 0.0)
+            return FPG_ERR_INVALID_RECEPTOR;
+    }
+    for (size_t i = 0; i < n_reg; ++i)
+        if (reg[i].lon_min > reg[i].lon_max || reg[i].lat_min > reg[i].lat_max || reg[i].z_min_m > reg[i].z_max_m)
+            return FPG_ERR_INVALID_SOURCE_BOUNDS;
+    // the driver over build_receptor_release_configs (timeloop.rs:1896-1917):
+    // each receptor a point release of all its particles at the start time
+    fpg_forward_config fc;
+    fpg_forward_config_default(&fc);
+    fc.start_seconds = cfg->start_seconds;
+    fc.end_seconds = cfg->end_seconds;
+    fc.timestep_seconds = cfg->timestep_seconds;
+    fc.clamp_time_bounds = cfg->clamp_time_bounds;
+    fc.x_grid_per_meter = cfg->x_grid_per_meter;
+    fc.y_grid_per_meter = cfg->y_grid_per_meter;
+    fc.z_grid_per_meter = cfg->z_grid_per_meter;
+    fc.pbl_options = cfg->pbl_options;
+    fc.dry_reference_height_m = cfg->dry_reference_height_m;
+    std::memcpy(fc.philox_key, cfg->philox_key, sizeof(fc.philox_key));
+    std::memcpy(fc.initial_philox_counter, cfg->initial_philox_counter, sizeof(fc.initial_philox_counter));
+    fc.sort_interval_steps = 0;
+    fc.use_compaction = 0;
+    fc.n_substeps = cfg->n_substeps;
+    fc.min_height_m = cfg->min_height_m;
+    std::vector<fpg_release> rel(n_rec);
+    for (size_t i = 0; i < n_rec; ++i) {
+        fpg_release& r = rel[i];
+        r.start_seconds = r.end_seconds = cfg->start_seconds;
+        r.lon_min = r.lon_max = rec[i].lon;
+        r.lat_min = r.lat_max = rec[i].lat;
+        r.z_min = r.z_max = rec[i].z_m;
+        r.mass_kg = rec[i].mass_kg;
+        r.particle_count = rec[i].particle_count;
+    }
+    fpg_backward* b = new fpg_backward();
+    fpg_status st = driver_create(ctx, &fc, rel.data(), n_rec, grid, capacity, nx, ny, nz, heights, -1, &b->f);
+    if (st != FPG_OK) {
+        delete b;
+        return st;
+    }
+    for (size_t i = 0; i < n_reg; ++i)
+        b->regions.push_back(RegionBox{reg[i].lon_min, reg[i].lon_max, reg[i].lat_min, reg[i].lat_max,
+                                       reg[i].z_min_m, reg[i].z_max_m});
+    const size_t nr = std::max<size_t>(n_reg, 1);
+    cudaError_t e = cudaMalloc(&b->d_regions, nr * sizeof(RegionBox));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_hits, nr * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_mass, nr * sizeof(double));
+    if (e == cudaSuccess && n_reg)
+        e = cudaMemcpyAsync(b->d_regions, b->regions.data(), n_reg * sizeof(RegionBox), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        fpg_backward_destroy(b);
+        return cuda_status(e);
+    }
+    *out = b;
+    return FPG_OK;
+}
+
+extern "C" int32_t fpg_backward_has_remaining_steps(const fpg_backward* b) {
+    return b ? fpg_forward_has_remaining_steps(b->f) : 0;
+}
+extern "C" int64_t fpg_backward_current_time(const fpg_backward* b) { return b ? fpg_forward_current_time(b->f) : 0; }
+extern "C" fpg_particles* fpg_backward_particles(fpg_backward* b) { return b ? b->f->particles : nullptr; }
+
+extern "C" fpg_status fpg_backward_run_timestep(fpg_backward* b, const fpg_met_bracket* met, const fpg_forcing* f,
+                                                fpg_step_report* report, fpg_source_collection* out) {
+    if (!b) return FPG_ERR_INVALID_ARGUMENT;
+    fpg_status st = fpg_forward_run_timestep(b->f, met, f, report);
+    if (st != FPG_OK) return st;
+    fpg_forward* d = b->f;
+    cudaStream_t s = d->ctx->stream;
+    const size_t nr = b->regions.size();
+    if (nr) {
+        FPG_CUDA(cudaMemsetAsync(b->d_hits, 0, nr * sizeof(unsigned long long), s));
+        FPG_CUDA(cudaMemsetAsync(b->d_mass, 0, nr * sizeof(double), s));
+        const uint32_t n = (uint32_t)d->next_free;
+        if (n) {
+            fpg_particles* P = d->particles;
+            const uint32_t blocks = std::min<uint32_t>((n + 255u) / 256u, (uint32_t)d->ctx->sm_count * 8u);
+            region_collect_kernel<<<blocks, 256, 0, s>>>(
+                (const int32_t*)P->field[FPG_FIELD_CELL_X], (const int32_t*)P->field[FPG_FIELD_CELL_Y],
+                (const float*)P->field[FPG_FIELD_POS_X], (const float*)P->field[FPG_FIELD_POS_Y],
+                (const float*)P->field[FPG_FIELD_POS_Z], (const uint32_t*)P->field[FPG_FIELD_FLAGS],
+                (const float*)P->field[FPG_FIELD_MASS0], n, b->d_regions, (uint32_t)nr, d->domain, b->d_hits,
+                b->d_mass);
+            d->ctx->count();
+            FPG_CHECK_LAUNCH();
+        }
+    }
+    std::vector<unsigned long long> hits(nr);
+    std::vector<double> mass(nr);
+    if (nr) {
+        FPG_CUDA(cudaMemcpyAsync(hits.data(), b->d_hits, nr * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        FPG_CUDA(cudaMemcpyAsync(mass.data(), b->d_mass, nr * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    // the reference waits for the device every backward step (timeloop.rs:1798)
+    FPG_CUDA(cudaStreamSynchronize(s));
+    if (out)
+        for (size_t r = 0; r < nr; ++r) {
+            out[r].hit_count = hits[r];
+            out[r].total_mass_kg = (float)mass[r];
+            out[r].pad = 0.0f;
+            out[r].total_mass_kg_f64 = mass[r];
+        }
+    return FPG_OK;
 }

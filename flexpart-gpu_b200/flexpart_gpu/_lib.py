@@ -139,6 +139,13 @@ _sig("fpg_inverse_forward", _i32, _vp, _vp)
 _sig("fpg_inverse_backward", _i32, _vp, _vp, _vp, _vp, _vp)
 _sig("fpg_inverse_batch", _vp, _vp)
 _sig("fpg_inverse_device_bytes", ctypes.c_uint64, _vp)
+_sig("fpg_backward_config_default", None, _vp)
+_sig("fpg_backward_create", _i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _sz, _sz, _sz, _sz, _vp, ctypes.POINTER(_vp))
+_sig("fpg_backward_destroy", _i32, _vp)
+_sig("fpg_backward_has_remaining_steps", _i32, _vp)
+_sig("fpg_backward_current_time", ctypes.c_int64, _vp)
+_sig("fpg_backward_run_timestep", _i32, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_backward_particles", _vp, _vp)
 _sig("fpg_sorter_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
 _sig("fpg_sorter_destroy", _i32, _vp)
 _sig("fpg_sort_by_cell", _i32, _vp, _vp, _vp, _vp, _vp, _vp)
@@ -177,6 +184,8 @@ EXPORTED_DRIVER = [
     "fpg_forward_config_default", "fpg_forward_create", "fpg_forward_destroy", "fpg_forward_has_remaining_steps",
     "fpg_forward_current_time", "fpg_forward_run_timestep", "fpg_forward_finalize", "fpg_forward_particles",
     "fpg_forward_accumulate_grid", "fpg_parse_timestamp",
+    "fpg_backward_config_default", "fpg_backward_create", "fpg_backward_destroy", "fpg_backward_has_remaining_steps",
+    "fpg_backward_current_time", "fpg_backward_run_timestep", "fpg_backward_particles",
     "fpg_batch_create", "fpg_batch_destroy", "fpg_batch_upload_frame", "fpg_batch_run", "fpg_batch_run_sequential",
     "fpg_batch_steps_done", "fpg_batch_scenario_slots", "fpg_batch_particles", "fpg_batch_download_grids",
     "fpg_batch_errors", "fpg_batch_tuning_candidates", "fpg_batch_autotune", "fpg_batch_set_tuning",

@@ -221,6 +221,42 @@ class InverseConfig(ctypes.Structure):
                 ("checkpoint_every", ctypes.c_uint32)]
 
 
+class ReceptorRelease(ctypes.Structure):
+    """``fpg_receptor_release``: BackwardReceptorConfig (timeloop.rs:150-163)."""
+
+    _fields_ = [("lon", ctypes.c_double), ("lat", ctypes.c_double), ("z_m", ctypes.c_double),
+                ("particle_count", ctypes.c_uint64), ("mass_kg", ctypes.c_double)]
+
+
+class SourceRegion(ctypes.Structure):
+    """``fpg_source_region``: BackwardSourceRegionConfig (timeloop.rs:170-197)."""
+
+    _fields_ = [("lon_min", ctypes.c_double), ("lon_max", ctypes.c_double), ("lat_min", ctypes.c_double),
+                ("lat_max", ctypes.c_double), ("z_min_m", ctypes.c_double), ("z_max_m", ctypes.c_double)]
+
+
+class SourceCollection(ctypes.Structure):
+    """``fpg_source_collection``: BackwardSourceCollection (timeloop.rs:201-206)."""
+
+    _fields_ = [("hit_count", ctypes.c_uint64), ("total_mass_kg", ctypes.c_float), ("pad", ctypes.c_float),
+                ("total_mass_kg_f64", ctypes.c_double)]
+
+
+class BackwardConfig(ctypes.Structure):
+    """``fpg_backward_config``: BackwardTimeLoopConfig (timeloop.rs:226-251)."""
+
+    _fields_ = [
+        ("start_seconds", ctypes.c_int64), ("end_seconds", ctypes.c_int64), ("timestep_seconds", ctypes.c_int64),
+        ("clamp_time_bounds", ctypes.c_int32),
+        ("x_grid_per_meter", ctypes.c_float), ("y_grid_per_meter", ctypes.c_float),
+        ("z_grid_per_meter", ctypes.c_float),
+        ("pbl_options", PblOptions),
+        ("dry_reference_height_m", ctypes.c_float),
+        ("philox_key", ctypes.c_uint32 * 2), ("initial_philox_counter", ctypes.c_uint32 * 4),
+        ("n_substeps", ctypes.c_uint32), ("min_height_m", ctypes.c_float),
+    ]
+
+
 class MetBracket(ctypes.Structure):
     """``fpg_met_bracket``: MetTimeBracket (timeloop.rs:270-285)."""
 

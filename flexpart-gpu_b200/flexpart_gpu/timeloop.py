@@ -14,6 +14,7 @@ from . import synthetic
 from ._lib import check, lib
 from .api import Context, Grid, Particles
 from .records import (
+    BackwardConfig,
     FORCING_NONE,
     FORCING_PER_CELL,
     FORCING_UNIFORM,
@@ -22,7 +23,10 @@ from .records import (
     GridDomain,
     MetBracket,
     PblOptions,
+    ReceptorRelease,
     Release,
+    SourceCollection,
+    SourceRegion,
     StepReport,
 )
 
@@ -95,6 +99,69 @@ class ForwardDriver:
         check(lib.fpg_forward_accumulate_grid(self.h, grid.h, species, mass_scale, _p(oh),
                                               0 if oh is None else oh.size), "fpg_forward_accumulate_grid")
         return grid.download()
+
+
+class BackwardDriver:
+    """Backward (receptor) mode behind the C ABI, in the shape of the
+    reference's BackwardTimeLoopDriver (src/simulation/timeloop.rs:1433-1909):
+    ``run_timestep(met, forcing)`` returns the step report and, per source
+    region, (hit_count, total_mass_kg, total_mass_kg_f64)."""
+
+    def __init__(self, ctx: Context, config: BackwardConfig, receptors, regions, grid: GridDomain, capacity: int,
+                 met_shape, level_heights=None):
+        self.ctx = ctx
+        self.config = config
+        rec = (ReceptorRelease * max(len(receptors), 1))(*receptors)
+        reg = (SourceRegion * max(len(regions), 1))(*regions)
+        self.n_regions = len(regions)
+        nx, ny, nz = met_shape
+        self._heights = None if level_heights is None else np.ascontiguousarray(level_heights, np.float32)
+        h = _vp()
+        check(lib.fpg_backward_create(ctx.h, ctypes.byref(config), rec, len(receptors), reg, len(regions),
+                                      ctypes.byref(grid), capacity, nx, ny, nz, _p(self._heights), ctypes.byref(h)),
+              "fpg_backward_create")
+        self.h = h
+        self.capacity = capacity
+
+    def __del__(self):
+        try:
+            if self.h and self.ctx.h:
+                lib.fpg_backward_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def has_remaining_steps(self) -> bool:
+        return bool(lib.fpg_backward_has_remaining_steps(self.h))
+
+    @property
+    def current_time_seconds(self) -> int:
+        return int(lib.fpg_backward_current_time(self.h))
+
+    @property
+    def particles(self) -> Particles:
+        return _ParticlesView(self.ctx, lib.fpg_backward_particles(self.h))
+
+    def run_timestep(self, met: MetBracket, forcing: Forcing):
+        rep = StepReport()
+        col = (SourceCollection * max(self.n_regions, 1))()
+        check(lib.fpg_backward_run_timestep(self.h, ctypes.byref(met), ctypes.byref(forcing), ctypes.byref(rep),
+                                            col), "fpg_backward_run_timestep")
+        return rep, [(int(c.hit_count), float(c.total_mass_kg), float(c.total_mass_kg_f64))
+                     for c in col[: self.n_regions]]
+
+
+def backward_config(**kw) -> BackwardConfig:
+    c = BackwardConfig()
+    lib.fpg_backward_config_default(ctypes.byref(c))
+    for k, v in kw.items():
+        if k in ("philox_key", "initial_philox_counter"):
+            arr = getattr(c, k)
+            for i, x in enumerate(v):
+                arr[i] = int(x) & 0xFFFFFFFF
+        else:
+            setattr(c, k, v)
+    return c
 
 
 def default_config(**kw) -> ForwardConfig:
@@ -174,5 +241,5 @@ def cell_forcing(cells, dry_velocity=0.0, rho_grad_over_rho=0.0) -> Forcing:
     return f
 
 
-__all__ = ["ForwardDriver", "default_config", "parse_timestamp", "scenario_releases", "scenario_domain",
+__all__ = ["ForwardDriver", "BackwardDriver", "backward_config", "default_config", "parse_timestamp", "scenario_releases", "scenario_domain",
            "scenario_config", "BracketSource", "uniform_forcing", "cell_forcing", "FORCING_NONE", "PblOptions"]

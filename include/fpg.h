@@ -64,6 +64,10 @@ enum {
     FPG_ERR_OUT_OF_GRID = -16,       /* ReleaseError::OutOfGridDomain: release/mod.rs:41 */
     FPG_ERR_TOO_MANY_LEVELS = -17,   /* more than FPG_MAX_LEVELS heights */
     FPG_ERR_INVALID_TIME_RANGE = -18, /* TimeLoopError::InvalidTimeRange: simulation/timeloop.rs:1935 */
+    FPG_ERR_INVALID_BACKWARD_TIME_RANGE = -19, /* TimeLoopError::InvalidBackwardTimeRange: simulation/timeloop.rs:1978 */
+    FPG_ERR_MISSING_RECEPTORS = -20, /* TimeLoopError::MissingReceptors: simulation/timeloop.rs:1994 */
+    FPG_ERR_INVALID_RECEPTOR = -21,  /* TimeLoopError::InvalidReceptor: simulation/timeloop.rs:2006-2046 */
+    FPG_ERR_INVALID_SOURCE_BOUNDS = -22, /* TimeLoopError::InvalidSourceBounds: simulation/timeloop.rs:2049-2073 */
     FPG_ERR_CUDA = -100,             /* any CUDA runtime error (see fpg_last_cuda_error) */
     FPG_ERR_OUT_OF_MEMORY = -101,
     FPG_ERR_NO_DEVICE = -102

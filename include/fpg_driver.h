@@ -132,6 +132,85 @@ fpg_status fpg_forward_accumulate_grid(fpg_forward* d, fpg_grid* grid, uint32_t 
                                        float mass_scale, const float* outheights, size_t n_outheights);
 
 /* ------------------------------------------------------------------------
+ * Backward (receptor) mode: BackwardTimeLoopDriver
+ * (src/simulation/timeloop.rs:1433-1909).
+ *
+ * Receptors release their particles at the start time (later than the end
+ * time); the clock runs backward by timestep_seconds per step; each step is
+ * the fused step with advection at -dt and turbulence and deposition at +dt
+ * (timeloop.rs:1724-1768), the Philox counter advancing by capacity x
+ * blocks; after the step, the active particles inside each source region
+ * are counted and their species-0 mass summed (collect_source_collections,
+ * timeloop.rs:1865-1894) by one device pass.
+ * ---------------------------------------------------------------------- */
+
+/* BackwardReceptorConfig (timeloop.rs:150-163): a point release at (lon, lat,
+ * z_m) of particle_count particles carrying mass_kg in all. */
+typedef struct fpg_receptor_release {
+    double lon, lat, z_m;
+    uint64_t particle_count;
+    double mass_kg;
+} fpg_receptor_release;
+
+/* BackwardSourceRegionConfig (timeloop.rs:170-197): inclusive bounds;
+ * a particle's lon = xlon0 + (cell_x + pos_x) * dx in double, lat likewise. */
+typedef struct fpg_source_region {
+    double lon_min, lon_max;
+    double lat_min, lat_max;
+    double z_min_m, z_max_m;
+} fpg_source_region;
+
+/* BackwardSourceCollection (timeloop.rs:201-206).  total_mass_kg is the sum
+ * in double rounded to float (the reference adds floats in slot order, whose
+ * rounding depends on that order); total_mass_kg_f64 is the double sum. */
+typedef struct fpg_source_collection {
+    uint64_t hit_count;
+    float total_mass_kg;
+    float pad;
+    double total_mass_kg_f64;
+} fpg_source_collection;
+
+/* BackwardTimeLoopConfig (timeloop.rs:226-251). */
+typedef struct fpg_backward_config {
+    int64_t start_seconds, end_seconds;   /* start >= end; both inclusive */
+    int64_t timestep_seconds;             /* > 0: the step magnitude */
+    int32_t clamp_time_bounds;            /* TimeBoundsBehavior: 1 Clamp, 0 Strict */
+    float x_grid_per_meter, y_grid_per_meter, z_grid_per_meter;
+    fpg_pbl_options pbl_options;
+    float dry_reference_height_m;         /* 15 m */
+    uint32_t philox_key[2];
+    uint32_t initial_philox_counter[4];
+    uint32_t n_substeps;                  /* 4 (timeloop.rs:1744) */
+    float min_height_m;                   /* 0.01 (timeloop.rs:1745) */
+} fpg_backward_config;
+
+/* The reference's defaults (timeloop.rs:253-270, the step of :1741-1746). */
+void fpg_backward_config_default(fpg_backward_config* cfg);
+
+typedef struct fpg_backward fpg_backward;
+
+/* BackwardTimeLoopDriver::new (timeloop.rs:1497-1571) with
+ * validate_backward_config (:1974-2073): FPG_ERR_INVALID_BACKWARD_TIME_RANGE,
+ * FPG_ERR_INVALID_TIME_STEP, FPG_ERR_INVALID_REFERENCE_HEIGHT,
+ * FPG_ERR_MISSING_RECEPTORS, FPG_ERR_INVALID_RECEPTOR (lon outside
+ * [-180, 180], lat outside [-90, 90], z < 0 or not finite, count 0, mass
+ * <= 0 or not finite), FPG_ERR_INVALID_SOURCE_BOUNDS (min > max). */
+fpg_status fpg_backward_create(fpg_ctx* ctx, const fpg_backward_config* cfg, const fpg_receptor_release* receptors,
+                               size_t n_receptors, const fpg_source_region* regions, size_t n_regions,
+                               const fpg_grid_domain* release_grid, size_t capacity, size_t met_nx, size_t met_ny,
+                               size_t met_nz, const float* level_heights, fpg_backward** out);
+fpg_status fpg_backward_destroy(fpg_backward* d);
+/* has_remaining_steps (timeloop.rs:1573-1577): current time >= end. */
+int32_t fpg_backward_has_remaining_steps(const fpg_backward* d);
+int64_t fpg_backward_current_time(const fpg_backward* d);
+/* run_timestep (timeloop.rs:1598-1821): release, alpha, bracket, PBL, the
+ * step at -dt / +dt, then the source collections (n_regions entries, may be
+ * NULL); waits for the device, as the reference does every backward step. */
+fpg_status fpg_backward_run_timestep(fpg_backward* d, const fpg_met_bracket* met, const fpg_forcing* forcing,
+                                     fpg_step_report* report, fpg_source_collection* collections);
+fpg_particles* fpg_backward_particles(fpg_backward* d);
+
+/* ------------------------------------------------------------------------
  * Batched ensemble: many independent release scenarios stepped together.
  *
  * No counterpart in the reference, which runs one scenario per driver.  Each

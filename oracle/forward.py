@@ -162,3 +162,72 @@ class OracleForward:
 
     def grid(self, species=0, mass_scale=1e6):
         return orc.grid(self.state, self.next_free, species, mass_scale, self.scn.outheights, self.scn.out_shape)
+
+
+class OracleBackward(OracleForward):
+    """BackwardTimeLoopDriver::run_timestep (src/simulation/timeloop.rs:
+    1598-1821) over the oracle: receptors are point releases at the start
+    time (build_receptor_release_configs, :1896-1917), the clock runs back by
+    dt, advection takes -dt while turbulence and deposition take +dt
+    (:1724-1746), the counter advances by capacity x blocks, and after the
+    step collect_source_collections (:1865-1894) counts the active particles
+    inside each region and sums their species-0 mass (in float, slot order,
+    as the reference; and in double).  `bracket(t)` gives (frame t0, frame t1,
+    time t0, time t1) for the step's time."""
+
+    def __init__(self, scn, capacity, frames, regions, bracket, **kw):
+        super().__init__(scn, capacity, frames, **kw)
+        self.regions = regions
+        self.bracket = bracket
+
+    @property
+    def has_remaining_steps(self):
+        return self.t >= self.scn.end
+
+    def collections(self):
+        spec = self.scn.met
+        n = self.next_free
+        st = self.state
+        act = (st.flags[:n] & 1) != 0
+        lon = spec.xlon0 + (st.cell_x[:n].astype(np.float64) + st.pos_x[:n].astype(np.float32).astype(np.float64)) * spec.dx_deg
+        lat = spec.ylat0 + (st.cell_y[:n].astype(np.float64) + st.pos_y[:n].astype(np.float32).astype(np.float64)) * spec.dy_deg
+        z = st.pos_z[:n].astype(np.float32).astype(np.float64)
+        m32 = st.mass[0, :n].astype(np.float32)
+        out = []
+        for r in self.regions:
+            hit = act & (lon >= r["lon_min"]) & (lon <= r["lon_max"]) & (lat >= r["lat_min"]) & \
+                (lat <= r["lat_max"]) & (z >= r["z_min_m"]) & (z <= r["z_max_m"])
+            s32 = np.float32(0.0)
+            for v in m32[hit]:
+                s32 = np.float32(s32 + v)
+            out.append((int(hit.sum()), float(s32), float(m32[hit].astype(np.float64).sum())))
+        return out
+
+    def run_timestep(self, forcing: dict, wet_cells=None):
+        from flexpart_gpu.records import StepParams
+
+        scn = self.scn
+        released = self._release(self.t)
+        f0, f1, ta, tb = self.bracket(self.t)
+        st, alpha = orc.interpolation_alpha(ta, tb, self.t, True)
+        assert st == 0
+        pbl = orc.pbl_diagnostics(f0["surface"], f1["surface"], alpha, scn.met.nx, scn.met.ny, dtype=self.dtype)
+        met = {"u0": f0["u"], "v0": f0["v"], "w0": f0["w"], "u1": f1["u"], "v1": f1["v"], "w1": f1["w"],
+               "heights": self.heights}
+        dry = forcing.get("dry_velocity", 0.0)
+        prm = StepParams.production(alpha=alpha, dt_seconds=-float(scn.dt), turb_dt_seconds=float(scn.dt),
+                                    x_grid_per_meter=self.xs, y_grid_per_meter=self.ys, z_grid_per_meter=self.zs,
+                                    key=self.key, counter=self.counter, n_substeps=self.n_substeps,
+                                    rho_grad_over_rho=forcing.get("rho_grad_over_rho", 0.0),
+                                    dry_mode=0 if dry == 0.0 else 1, dry_velocity_m_s=dry,
+                                    wet_mode=3 if wet_cells is not None else 0)
+        kw = {}
+        if wet_cells is not None:
+            kw = dict(wet_cells_lf=wet_cells, wet_shape=(scn.met.nx, scn.met.ny))
+        orc.step(self.state, self.next_free, met, pbl, prm, threads=self.threads, **kw)
+        self.counter = orc.next_counter(self.counter, self.capacity, self.n_substeps)
+        self.step_index += 1
+        t = self.t
+        self.t -= scn.dt
+        return {"time": t, "alpha": alpha, "released": released, "active": self.active,
+                "counter": list(self.counter), "collections": self.collections()}

@@ -57,6 +57,8 @@ def test_record_layouts_match_the_c_header(tmp_path):
         "fpg_grid_domain": R.GridDomain, "fpg_forward_config": R.ForwardConfig, "fpg_met_bracket": R.MetBracket,
         "fpg_forcing": R.Forcing, "fpg_step_report": R.StepReport, "fpg_batch_scenario": R.BatchScenario,
         "fpg_batch_tuning": R.BatchTuning, "fpg_receptor": R.Receptor,
+        "fpg_receptor_release": R.ReceptorRelease, "fpg_source_region": R.SourceRegion,
+        "fpg_source_collection": R.SourceCollection, "fpg_backward_config": R.BackwardConfig,
         "fpg_inverse_config": R.InverseConfig,
         "fpg_batch_config": R.BatchConfig,
     }
