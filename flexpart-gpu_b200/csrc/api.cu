@@ -166,6 +166,19 @@ extern "C" fpg_status fpg_device_free(fpg_ctx* c, void* ptr) {
     return FPG_OK;
 }
 
+extern "C" fpg_status fpg_host_alloc(fpg_ctx* c, size_t bytes, void** out) {
+    if (!c || !out) return FPG_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    FPG_CUDA(cudaHostAlloc(out, bytes > 0 ? bytes : 4, cudaHostAllocDefault));
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_host_free(fpg_ctx* c, void* ptr) {
+    if (!c) return FPG_ERR_INVALID_ARGUMENT;
+    if (ptr) FPG_CUDA(cudaFreeHost(ptr));
+    return FPG_OK;
+}
+
 extern "C" fpg_status fpg_memcpy(fpg_ctx* c, void* dst, const void* src, size_t bytes, int32_t kind, void* stream) {
     if (!c || ((!dst || !src) && bytes) || kind < 0 || kind > 2) return FPG_ERR_INVALID_ARGUMENT;
     if (bytes == 0) return FPG_OK;

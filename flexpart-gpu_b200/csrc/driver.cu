@@ -95,6 +95,19 @@ struct fpg_forward {
     // +1 forward; -1 backward (BackwardTimeLoopDriver): the clock runs back,
     // advection takes -dt and turbulence/deposition +dt (timeloop.rs:1724-1746)
     int direction = 1;
+    // met streaming: frames copied ahead on copy_stream into ring slots
+    struct MetSlot {
+        int64_t time = 0;
+        bool valid = false;
+        uint64_t last_use = 0;
+        float* uvw = nullptr;                 // 3 * nodes
+        fpg_surface_cell* surface = nullptr;  // nx * ny
+        cudaEvent_t copied = nullptr;         // recorded on copy_stream after the copy
+        cudaEvent_t released = nullptr;       // recorded on the step stream after the last read
+    };
+    std::vector<MetSlot> ring;
+    cudaStream_t copy_stream = nullptr;
+    uint64_t tick = 0, ring_hits = 0, host_uploads = 0;
 };
 
 using namespace fpg;
@@ -143,6 +156,16 @@ extern "C" fpg_status fpg_forward_destroy(fpg_forward* d) {
     fpg_compaction_destroy(d->compaction);
     fpg_sorter_destroy(d->sorter);
     for (float* p : d->d_forcing) cudaFree(p);
+    for (auto& slot : d->ring) {
+        cudaFree(slot.uvw);
+        cudaFree(slot.surface);
+        if (slot.copied) cudaEventDestroy(slot.copied);
+        if (slot.released) cudaEventDestroy(slot.released);
+    }
+    if (d->copy_stream) {
+        cudaStreamSynchronize(d->copy_stream);
+        cudaStreamDestroy(d->copy_stream);
+    }
     delete d;
     return FPG_OK;
 }
@@ -265,6 +288,37 @@ static fpg_status upload_forcing(fpg_forward* d, int k, const float* host) {
     return FPG_OK;
 }
 
+// The ring slot holding the frame valid at time t, or -1.
+static int ring_find(const fpg_forward* d, int64_t t) {
+    for (size_t i = 0; i < d->ring.size(); ++i)
+        if (d->ring[i].valid && d->ring[i].time == t) return (int)i;
+    return -1;
+}
+
+// Both frames of bracket (t0, t1) from the ring, packed on the step stream
+// after their copies; FPG_ERR_NOT_READY when either is missing.
+static fpg_status bracket_from_ring(fpg_forward* d, int64_t t0, int64_t t1) {
+    const int i0 = ring_find(d, t0), i1 = ring_find(d, t1);
+    if (i0 < 0 || i1 < 0) return FPG_ERR_NOT_READY;
+    cudaStream_t s = d->ctx->stream;
+    const size_t nodes = d->met->nx * d->met->ny * d->met->nz, cells = d->met->nx * d->met->ny;
+    const int idx[2] = {i0, i1};
+    for (int which = 0; which < 2; ++which) {
+        fpg_forward::MetSlot& slot = d->ring[idx[which]];
+        FPG_CUDA(cudaStreamWaitEvent(s, slot.copied, 0));
+        fpg_status st = fpg_met_upload_frame_device(d->met, which, slot.uvw, slot.uvw + nodes, slot.uvw + 2 * nodes,
+                                                    nullptr);
+        if (st != FPG_OK) return st;
+        FPG_CUDA(cudaMemcpyAsync(d->surface->frame[which], slot.surface, cells * sizeof(fpg_surface_cell),
+                                 cudaMemcpyDeviceToDevice, s));
+        d->surface->uploaded[which] = true;
+        slot.last_use = ++d->tick;
+    }
+    // the slots are not read after the repack: later copies into them wait for this
+    for (int which = 0; which < 2; ++which) FPG_CUDA(cudaEventRecord(d->ring[idx[which]].released, s));
+    return FPG_OK;
+}
+
 extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bracket* met, const fpg_forcing* f,
                                                fpg_step_report* report) {
     if (!d || !met || !f) return FPG_ERR_INVALID_ARGUMENT;
@@ -296,6 +350,17 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
 
     // upload_dual_wind_if_bracket_changed (timeloop.rs:1378-1402) + surface frames
     if (!d->have_bracket || d->bracket_t0 != t0 || d->bracket_t1 != t1) {
+        if ((st = bracket_from_ring(d, t0, t1)) == FPG_OK) {
+            d->ring_hits += 1;
+            d->have_bracket = true;
+            d->bracket_t0 = t0;
+            d->bracket_t1 = t1;
+        } else if (st != FPG_ERR_NOT_READY) {
+            return st;
+        }
+    }
+    if (!d->have_bracket || d->bracket_t0 != t0 || d->bracket_t1 != t1) {
+        d->host_uploads += 1;
         if (!met->wind_t0_u || !met->wind_t0_v || !met->wind_t0_w || !met->wind_t1_u || !met->wind_t1_v ||
             !met->wind_t1_w || !met->surface_t0 || !met->surface_t1)
             return FPG_ERR_INVALID_ARGUMENT;
@@ -396,6 +461,57 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
     }
     d->step_index += 1;
     d->t += d->direction > 0 ? d->cfg.timestep_seconds : -d->cfg.timestep_seconds;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_met_ring(fpg_forward* d, uint32_t n_slots) {
+    if (!d || n_slots < 2) return FPG_ERR_INVALID_ARGUMENT;
+    if (!d->ring.empty()) return d->ring.size() == n_slots ? FPG_OK : FPG_ERR_INVALID_ARGUMENT;
+    const size_t nodes = d->met->nx * d->met->ny * d->met->nz, cells = d->met->nx * d->met->ny;
+    cudaError_t e = cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking);
+    d->ring.resize(n_slots);
+    for (auto& slot : d->ring) {
+        if (e == cudaSuccess) e = cudaMalloc(&slot.uvw, 3 * nodes * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&slot.surface, cells * sizeof(fpg_surface_cell));
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.copied, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.released, cudaEventDisableTiming);
+    }
+    return e == cudaSuccess ? FPG_OK : cuda_status(e);
+}
+
+extern "C" fpg_status fpg_forward_prefetch_frame(fpg_forward* d, int64_t t, const float* u, const float* v,
+                                                 const float* w, const fpg_surface_cell* surface) {
+    if (!d || !u || !v || !w || !surface) return FPG_ERR_INVALID_ARGUMENT;
+    if (d->ring.empty()) return FPG_ERR_NOT_READY;
+    if (ring_find(d, t) >= 0) return FPG_OK;
+    // victim: a free slot, else the least recently used outside the current bracket
+    int victim = -1;
+    for (size_t i = 0; i < d->ring.size(); ++i) {
+        const fpg_forward::MetSlot& slot = d->ring[i];
+        if (!slot.valid) { victim = (int)i; break; }
+        if (d->have_bracket && (slot.time == d->bracket_t0 || slot.time == d->bracket_t1)) continue;
+        if (victim < 0 || slot.last_use < d->ring[victim].last_use) victim = (int)i;
+    }
+    if (victim < 0) return FPG_ERR_STORE_FULL;
+    fpg_forward::MetSlot& slot = d->ring[victim];
+    const size_t nodes = d->met->nx * d->met->ny * d->met->nz, cells = d->met->nx * d->met->ny;
+    cudaStream_t cs = d->copy_stream;
+    FPG_CUDA(cudaStreamWaitEvent(cs, slot.released, 0));
+    FPG_CUDA(cudaMemcpyAsync(slot.uvw, u, nodes * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FPG_CUDA(cudaMemcpyAsync(slot.uvw + nodes, v, nodes * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FPG_CUDA(cudaMemcpyAsync(slot.uvw + 2 * nodes, w, nodes * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FPG_CUDA(cudaMemcpyAsync(slot.surface, surface, cells * sizeof(fpg_surface_cell), cudaMemcpyHostToDevice, cs));
+    FPG_CUDA(cudaEventRecord(slot.copied, cs));
+    slot.valid = true;
+    slot.time = t;
+    slot.last_use = ++d->tick;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_met_ring_stats(const fpg_forward* d, uint64_t* hits, uint64_t* uploads) {
+    if (!d) return FPG_ERR_INVALID_ARGUMENT;
+    if (hits) *hits = d->ring_hits;
+    if (uploads) *uploads = d->host_uploads;
     return FPG_OK;
 }
 

@@ -146,6 +146,11 @@ _sig("fpg_backward_has_remaining_steps", _i32, _vp)
 _sig("fpg_backward_current_time", ctypes.c_int64, _vp)
 _sig("fpg_backward_run_timestep", _i32, _vp, _vp, _vp, _vp, _vp)
 _sig("fpg_backward_particles", _vp, _vp)
+_sig("fpg_forward_met_ring", _i32, _vp, _u32)
+_sig("fpg_forward_prefetch_frame", _i32, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp)
+_sig("fpg_forward_met_ring_stats", _i32, _vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64))
+_sig("fpg_host_alloc", _i32, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_host_free", _i32, _vp, _vp)
 _sig("fpg_sorter_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
 _sig("fpg_sorter_destroy", _i32, _vp)
 _sig("fpg_sort_by_cell", _i32, _vp, _vp, _vp, _vp, _vp, _vp)
@@ -160,7 +165,7 @@ def check(status: int, what: str) -> None:
 EXPORTED = [
     "fpg_status_string", "fpg_last_cuda_error", "fpg_abi_version",
     "fpg_ctx_create", "fpg_ctx_destroy", "fpg_ctx_stream", "fpg_ctx_synchronize", "fpg_ctx_kernel_launches",
-    "fpg_device_alloc", "fpg_device_free", "fpg_memcpy", "fpg_memset",
+    "fpg_device_alloc", "fpg_device_free", "fpg_memcpy", "fpg_memset", "fpg_host_alloc", "fpg_host_free",
     "fpg_particles_create", "fpg_particles_destroy", "fpg_particles_capacity", "fpg_particles_dispatch_count",
     "fpg_particles_set_dispatch_count", "fpg_particles_upload", "fpg_particles_upload_slots",
     "fpg_particles_download", "fpg_particles_field", "fpg_particles_copy_field",
@@ -184,6 +189,7 @@ EXPORTED_DRIVER = [
     "fpg_forward_config_default", "fpg_forward_create", "fpg_forward_destroy", "fpg_forward_has_remaining_steps",
     "fpg_forward_current_time", "fpg_forward_run_timestep", "fpg_forward_finalize", "fpg_forward_particles",
     "fpg_forward_accumulate_grid", "fpg_parse_timestamp",
+    "fpg_forward_met_ring", "fpg_forward_prefetch_frame", "fpg_forward_met_ring_stats",
     "fpg_backward_config_default", "fpg_backward_create", "fpg_backward_destroy", "fpg_backward_has_remaining_steps",
     "fpg_backward_current_time", "fpg_backward_run_timestep", "fpg_backward_particles",
     "fpg_batch_create", "fpg_batch_destroy", "fpg_batch_upload_frame", "fpg_batch_run", "fpg_batch_run_sequential",

@@ -94,6 +94,26 @@ class ForwardDriver:
     def finalize(self):
         check(lib.fpg_forward_finalize(self.h), "fpg_forward_finalize")
 
+    def enable_met_ring(self, n_slots: int = 3):
+        """Met streaming: a device ring of n_slots frames filled ahead of use."""
+        check(lib.fpg_forward_met_ring(self.h, n_slots), "fpg_forward_met_ring")
+
+    def prefetch_frame(self, time_seconds: int, u, v, w, surface):
+        """Queues the copy of the met frame valid at time_seconds; the host
+        arrays must stay unchanged until the frame is used."""
+        self._keep.append((u, v, w, surface))
+        if len(self._keep) > 16:
+            del self._keep[:-16]
+        ptr = lambda a: ctypes.c_void_p(a.ctypes.data) if hasattr(a, "ctypes") else ctypes.c_void_p(int(a))
+        check(lib.fpg_forward_prefetch_frame(self.h, time_seconds, ptr(u), ptr(v), ptr(w), ptr(surface)),
+              "fpg_forward_prefetch_frame")
+
+    def met_ring_stats(self):
+        hits, uploads = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib.fpg_forward_met_ring_stats(self.h, ctypes.byref(hits), ctypes.byref(uploads)),
+              "fpg_forward_met_ring_stats")
+        return int(hits.value), int(uploads.value)
+
     def accumulate_concentration_grid(self, grid: Grid, species=0, mass_scale=1.0e6, outheights=None):
         oh = None if outheights is None else np.ascontiguousarray(outheights, np.float32)
         check(lib.fpg_forward_accumulate_grid(self.h, grid.h, species, mass_scale, _p(oh),

@@ -149,6 +149,11 @@ fpg_status fpg_device_alloc(fpg_ctx* ctx, size_t bytes, void** out);
 fpg_status fpg_device_free(fpg_ctx* ctx, void* ptr);
 fpg_status fpg_memcpy(fpg_ctx* ctx, void* dst, const void* src, size_t bytes, int32_t kind, void* stream);
 fpg_status fpg_memset(fpg_ctx* ctx, void* dst, int32_t value, size_t bytes, void* stream);
+/* Page-locked host memory: copies from it to the device run asynchronously
+ * and overlap kernels (fpg_forward_prefetch_frame streams met frames from
+ * such buffers). */
+fpg_status fpg_host_alloc(fpg_ctx* ctx, size_t bytes, void** out);
+fpg_status fpg_host_free(fpg_ctx* ctx, void* ptr);
 
 /* ------------------------------------------------------------------------
  * Particles (ParticleBuffers, src/gpu/buffers.rs:377-510)

@@ -131,6 +131,28 @@ fpg_particles* fpg_forward_particles(fpg_forward* d);
 fpg_status fpg_forward_accumulate_grid(fpg_forward* d, fpg_grid* grid, uint32_t species_index,
                                        float mass_scale, const float* outheights, size_t n_outheights);
 
+/* Met streaming, the device side of the reference's prefetching met reader
+ * (io/grib2_async.rs:41-120 feeding MetTimeBracket): a ring of n_slots met
+ * frames (u, v, w and surface cells) on the device, filled ahead of use on a
+ * separate copy stream.  fpg_forward_prefetch_frame queues the copy of the
+ * frame valid at time_seconds and returns without waiting (page-locked host
+ * buffers, fpg_host_alloc, make the copy overlap the steps; the host
+ * buffers must stay unchanged until the frame is used).  When run_timestep
+ * meets a new bracket whose two frames are in the ring, it repacks them on
+ * the device after their copies (no host copy, the bracket's host pointers
+ * are not read); otherwise it uploads from the bracket's host pointers as
+ * before.  A full ring evicts its least recently used frame outside the
+ * current bracket (after the repack that read it), so with n_slots = 3 the
+ * frame after the current bracket is prefetched once that bracket is in use
+ * (after its first run_timestep).  n_slots >= 2; the ring is kept for the
+ * driver's life.  Results do not depend on whether frames come from the
+ * ring. */
+fpg_status fpg_forward_met_ring(fpg_forward* d, uint32_t n_slots);
+fpg_status fpg_forward_prefetch_frame(fpg_forward* d, int64_t time_seconds, const float* u, const float* v,
+                                      const float* w, const fpg_surface_cell* surface);
+/* Brackets served from the ring and from host pointers so far. */
+fpg_status fpg_forward_met_ring_stats(const fpg_forward* d, uint64_t* ring_hits, uint64_t* host_uploads);
+
 /* ------------------------------------------------------------------------
  * Backward (receptor) mode: BackwardTimeLoopDriver
  * (src/simulation/timeloop.rs:1433-1909).

@@ -132,3 +132,51 @@ def test_driver_errors(ctx):
         for _ in range(5):
             drv2.run_timestep(src.at(drv2.current_time_seconds), tl.uniform_forcing())
     assert e.value.status == -9      # StoreFull (particles/mod.rs:516)
+
+
+def _run_with_ring(ctx, scn, frames, mode):
+    """24 h over 3 h brackets; mode "host": frames from the bracket's host
+    pointers; "ring": every frame prefetched a bracket ahead; "mixed": only
+    the frames of every other bracket prefetched, so half the brackets miss
+    the ring and fall back to the host pointers."""
+    drv = _driver(ctx, scn)
+    src = tl.BracketSource(scn, frames)
+    forcing = tl.uniform_forcing(dry_velocity=scn.dry_velocity)
+    fs = scn.met.frame_seconds
+    if mode != "host":
+        drv.enable_met_ring(3)
+    prefetched = set()
+
+    def prefetch(tf):
+        if tf not in prefetched:
+            f = src.frames[((tf - scn.start) // fs) % scn.met.n_frames]
+            drv.prefetch_frame(tf, f["u"], f["v"], f["w"], f["surface"])
+            prefetched.add(tf)
+
+    while drv.has_remaining_steps:
+        t = drv.current_time_seconds
+        _, _, ta, tb = synthetic.bracket_frames(scn, t)
+        if mode == "ring" and t == scn.start:
+            prefetch(ta)
+            prefetch(tb)
+        if mode == "mixed" and ((ta - scn.start) // fs) % 2 == 0:
+            prefetch(ta)
+            prefetch(tb)
+        drv.run_timestep(src.at(t), forcing)
+        if mode == "ring":
+            prefetch(tb + fs)      # the next bracket's new frame, once this bracket is in use
+    drv.finalize()
+    return drv.particles.download(), drv.met_ring_stats()
+
+
+def test_met_ring_streaming_gives_identical_results(ctx):
+    scn = _small(particles=20_000, hours=24)
+    frames = synthetic.make_frames(scn.met)
+    host, (h0, u0) = _run_with_ring(ctx, scn, frames, "host")
+    ring, (h1, u1) = _run_with_ring(ctx, scn, frames, "ring")
+    mixed, (h2, u2) = _run_with_ring(ctx, scn, frames, "mixed")
+    brackets = 8          # 24 h of 3 h brackets
+    assert (h0, u0) == (0, brackets)
+    assert (h1, u1) == (brackets, 0)
+    assert (h2, u2) == (brackets // 2, brackets // 2)
+    assert host.tobytes() == ring.tobytes() == mixed.tobytes()
