@@ -180,3 +180,25 @@ def test_met_ring_streaming_gives_identical_results(ctx):
     assert (h1, u1) == (brackets, 0)
     assert (h2, u2) == (brackets // 2, brackets // 2)
     assert host.tobytes() == ring.tobytes() == mixed.tobytes()
+
+
+def test_device_grid_written_as_netcdf_snapshot(ctx, tmp_path):
+    from scipy.io import netcdf_file
+
+    from flexpart_gpu import output
+
+    scn = _small(particles=20_000, hours=2)
+    frames = synthetic.make_frames(scn.met)
+    drv = _driver(ctx, scn)
+    src = tl.BracketSource(scn, frames)
+    while drv.has_remaining_steps:
+        drv.run_timestep(src.at(drv.current_time_seconds), tl.uniform_forcing(dry_velocity=0.002))
+    grid = api.Grid(ctx, *scn.out_shape)
+    counts, mass, kg = drv.accumulate_concentration_grid(grid, 0, 1e6, scn.outheights)
+    path = tmp_path / "grid.nc"
+    output.write_grid_netcdf(path, grid, scn.end)
+    with netcdf_file(path, "r", mmap=False) as f:
+        assert np.array_equal(f.variables["concentration_particle_count"][:].reshape(-1), counts.astype(np.int32))
+        assert np.array_equal(f.variables["concentration_mass_kg"][:].reshape(-1), kg)
+        assert f.variables["time"][0] == scn.end
+    assert counts.sum() == 20_000
