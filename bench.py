@@ -11,7 +11,7 @@ the real population of 10 M active particles spread along the plumes.
 One timed step = one 900 s sync step over all 10 M particles: met-bracket
 refresh at bracket changes (every 12 steps, from a device-resident frame
 ring), per-cell wet forcing at bracket changes, per-cell PBL diagnostics, a
-spatial reorder by met cell every 8 steps, the fused advection +
+spatial reorder by met cell every 12 steps, the fused advection +
 Hanna/Langevin + dry + wet kernel, and the concentration grid at each 3-hourly
 output time.  The particle state (960 MB) is larger than L2.
 
@@ -55,7 +55,7 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s"
 UNIT = "particle-steps/s"
 BYTES_PER_PARTICLE_STEP = 96  # read 44 B + write 52 B of SoA state, one species
-SORT_EVERY = 8
+SORT_EVERY = 12  # steps between spatial reorders (divides the default 24 timed steps after 4 warm-up)
 # DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
 # an ncu capture of a 2 M-particle launch (129.8 MB), scaled by the particle
 # count; below the algorithmic 96 B because part of the state was still in
@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-scenarios", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--sort-every", type=int, default=SORT_EVERY,
+                    help="steps between spatial reorders of the population")
     ap.add_argument("--adjoint-instances", type=int, default=64)
     ap.add_argument("--quick", action="store_true",
                     help="profiling case: no spin-up (particles scattered around the sources), no e2e, no CPU leg")
@@ -563,7 +565,7 @@ def main():
             set_bracket(fa, fb)
             state["bracket"] = (fa, fb, ta)
         alpha = (t - ta) / float(tb - ta)
-        if state["k"] % SORT_EVERY == 0:
+        if state["k"] % args.sort_every == 0:
             sorter.sort(parts, met)
         api.pbl_diagnostics(ctx, surf, alpha, pbl)
         prm = StepParams.production(alpha=alpha, dt_seconds=float(scn.dt), turb_dt_seconds=float(scn.dt),
@@ -719,7 +721,7 @@ def main():
                                    "(spun up), met 360x180x60, 9 frames 3 h apart, wet scavenging on, dt 900 s, "
                                    "output 360x180x5 every 3 h",
                        "particles_per_gpu": n_active, "met": [spec.nx, spec.ny, spec.nz],
-                       "sort_every_steps": SORT_EVERY, "spin_up_s": round(spin_s, 1),
+                       "sort_every_steps": args.sort_every, "spin_up_s": round(spin_s, 1),
                        "l2": "inputs larger than L2 (960 MB particle state per step)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE_NCU * n_active,

@@ -171,7 +171,7 @@ const StepVariant kVariants[] = {
     {256, 4, 1, batch_step_kernel<256, 4, 1>}, {256, 4, 2, batch_step_kernel<256, 4, 2>},
     {256, 3, 1, batch_step_kernel<256, 3, 1>}, {256, 2, 1, batch_step_kernel<256, 2, 1>},
     {128, 8, 1, batch_step_kernel<128, 8, 1>}, {128, 8, 2, batch_step_kernel<128, 8, 2>},
-    {512, 2, 1, batch_step_kernel<512, 2, 1>},
+    {512, 2, 1, batch_step_kernel<512, 2, 1>}, {256, 5, 1, batch_step_kernel<256, 5, 1>},
 };
 static_assert(sizeof(kVariants) / sizeof(kVariants[0]) == kNumVariants, "launch shape table");
 

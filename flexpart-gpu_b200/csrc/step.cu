@@ -34,7 +34,7 @@
 
 namespace fpg {
 
-__global__ void __launch_bounds__(256, 4) fused_step_kernel(StepArgs a) {
+__global__ void __launch_bounds__(256, 5) fused_step_kernel(StepArgs a) {
     extern __shared__ float s_heights[];
     if (a.stages & FPG_STAGE_ADVECT) {
         for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
