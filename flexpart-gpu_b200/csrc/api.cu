@@ -105,6 +105,10 @@ extern "C" const char* fpg_status_string(fpg_status s) {
         case FPG_ERR_MISSING_RECEPTORS: return "backward run needs at least one receptor";
         case FPG_ERR_INVALID_RECEPTOR: return "invalid receptor";
         case FPG_ERR_INVALID_SOURCE_BOUNDS: return "invalid source region bounds";
+        case FPG_ERR_NON_STOCHASTIC_COLUMN: return "convection matrix column is not stochastic";
+        case FPG_ERR_TOO_FEW_LEVELS: return "need at least 2 level interfaces";
+        case FPG_ERR_NON_MONOTONIC_INTERFACES: return "level interfaces must be finite and strictly increasing";
+        case FPG_ERR_INVALID_BOUNDARY_LAYER_HEIGHT: return "invalid boundary-layer height";
         case FPG_ERR_CUDA: return "CUDA error";
         case FPG_ERR_OUT_OF_MEMORY: return "out of device memory";
         case FPG_ERR_NO_DEVICE: return "no CUDA device";

@@ -106,6 +106,17 @@ _sig("fpg_compaction_destroy", _i32, _vp)
 _sig("fpg_compact", _i32, _vp, _vp, _vp, _u32p, _vp, _vp)
 _sig("fpg_philox_uniforms", _i32, _vp, _u32p, _u32p, _sz, _vp, _vp, _vp)
 _sig("fpg_compaction_indices_static", _i32, _vp, _vp, _sz, _vp, _vp, _vp)
+_sig("fpg_dispatch_hanna_params", _i32, _vp, _vp, _vp, _vp, _sz, _vp)
+_sig("fpg_cbl_sample", _i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp)
+_sig("fpg_cbl_sample_philox", _i32, _vp, _vp, _vp, _u32p, _u32p, _vp, _vp)
+_sig("fpg_convection_build_chain", _i32, _vp, _f32, _vp, _vp, _vp, _vp, _vp)
+_sig("fpg_convection_level_index", _sz, _vp, _sz, _f32)
+_sig("fpg_convection_apply_profile", _i32, _vp, _sz, _vp, _sz, _vp)
+_sig("fpg_convection_create", _i32, _vp, _sz, ctypes.POINTER(_vp))
+_sig("fpg_convection_destroy", _i32, _vp)
+_sig("fpg_convection_set_matrix", _i32, _vp, _vp, _sz, _vp, _sz, _vp)
+_sig("fpg_convection_heights", _i32, _vp, _vp)
+_sig("fpg_convective_mixing", _i32, _vp, _vp, _vp, _vp)
 _sig("fpg_forward_config_default", None, _vp)
 _sig("fpg_parse_timestamp", _i32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64))
 _sig("fpg_forward_create", _i32, _vp, _vp, _vp, _sz, _vp, _sz, _sz, _sz, _sz, _vp, ctypes.POINTER(_vp))
@@ -182,6 +193,10 @@ EXPORTED = [
     "fpg_philox_uniforms",
     "fpg_compaction_indices_static",
     "fpg_sorter_create", "fpg_sorter_destroy", "fpg_sort_by_cell",
+    "fpg_dispatch_hanna_params", "fpg_cbl_sample", "fpg_cbl_sample_philox",
+    "fpg_convection_build_chain", "fpg_convection_level_index", "fpg_convection_apply_profile",
+    "fpg_convection_create", "fpg_convection_destroy", "fpg_convection_set_matrix", "fpg_convection_heights",
+    "fpg_convective_mixing",
 ]
 
 # Every symbol include/fpg_driver.h declares.

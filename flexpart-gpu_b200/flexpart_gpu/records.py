@@ -28,6 +28,21 @@ PARTICLE_DTYPE = np.dtype(
 )
 assert PARTICLE_DTYPE.itemsize == 96
 
+# HannaParams (src/pbl/mod.rs:23-57), fpg_hanna_params: 64 bytes per slot.
+HANNA_PARAMS_DTYPE = np.dtype([(n, "<f4") for n in (
+    "ust", "wst", "ol", "h", "zeta", "sigu", "sigv", "sigw", "dsigwdz", "dsigw2dz", "tlu", "tlv", "tlw")]
+    + [("pad", "<f4", (3,))])
+assert HANNA_PARAMS_DTYPE.itemsize == 64
+
+# CblSamplingInput / CblSamplingOutput (src/gpu/cbl.rs:38-92).
+CBL_INPUT_DTYPE = np.dtype([("branch_uniform", "<f4"), ("gaussian_uniform0", "<f4"),
+                            ("gaussian_uniform1", "<f4"), ("pad0", "<f4")])
+CBL_OUTPUT_DTYPE = np.dtype([(n, "<f4") for n in (
+    "sampled_w_m_s", "updraft_weight", "updraft_mean_m_s", "updraft_sigma_m_s", "downdraft_weight",
+    "downdraft_mean_m_s", "downdraft_sigma_m_s", "second_moment_w2", "third_moment_w3", "skewness",
+    "transition", "z_over_h")])
+assert CBL_INPUT_DTYPE.itemsize == 16 and CBL_OUTPUT_DTYPE.itemsize == 48
+
 SURFACE_DTYPE = np.dtype(
     [
         ("surface_pressure_pa", "<f4"), ("temperature_2m_k", "<f4"),
@@ -289,6 +304,26 @@ class StepReport(ctypes.Structure):
         ("interpolation_alpha", ctypes.c_float), ("released_count", ctypes.c_uint64),
         ("first_released_slot", ctypes.c_uint64), ("active_particle_count", ctypes.c_uint64),
         ("next_philox_counter", ctypes.c_uint32 * 4),
+    ]
+
+
+class ConvectionInputs(ctypes.Structure):
+    """fpg_convection_inputs: SimplifiedEmanuelInputs (physics/convection.rs:68-82)."""
+    _fields_ = [
+        ("level_interfaces_m", ctypes.c_void_p), ("n_interfaces", ctypes.c_size_t),
+        ("convective_precip_mm_h", ctypes.c_float), ("convective_velocity_scale_m_s", ctypes.c_float),
+        ("boundary_layer_height_m", ctypes.c_float), ("has_cape_override", ctypes.c_int32),
+        ("cape_override_j_kg", ctypes.c_float),
+    ]
+
+
+class ConvectionColumn(ctypes.Structure):
+    """fpg_convection_column: the scalars of SimplifiedEmanuelColumn plus the
+    matrix's mixing fraction (physics/convection.rs:111-154)."""
+    _fields_ = [
+        ("is_active", ctypes.c_int32), ("cape_j_kg", ctypes.c_float), ("cloud_base_level", ctypes.c_uint32),
+        ("cloud_top_level", ctypes.c_uint32), ("convective_timescale_s", ctypes.c_float),
+        ("mixing_fraction", ctypes.c_float),
     ]
 
 

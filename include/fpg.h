@@ -68,6 +68,10 @@ enum {
     FPG_ERR_MISSING_RECEPTORS = -20, /* TimeLoopError::MissingReceptors: simulation/timeloop.rs:1994 */
     FPG_ERR_INVALID_RECEPTOR = -21,  /* TimeLoopError::InvalidReceptor: simulation/timeloop.rs:2006-2046 */
     FPG_ERR_INVALID_SOURCE_BOUNDS = -22, /* TimeLoopError::InvalidSourceBounds: simulation/timeloop.rs:2049-2073 */
+    FPG_ERR_NON_STOCHASTIC_COLUMN = -23, /* ConvectionError::NonStochasticColumn: physics/convection.rs:196-218 */
+    FPG_ERR_TOO_FEW_LEVELS = -24,    /* ConvectionError::TooFewLevels: physics/convection.rs:86-90 */
+    FPG_ERR_NON_MONOTONIC_INTERFACES = -25, /* ConvectionError::NonMonotonicInterfaces: physics/convection.rs:92-98 */
+    FPG_ERR_INVALID_BOUNDARY_LAYER_HEIGHT = -26, /* ConvectionError::InvalidBoundaryLayerHeight: physics/convection.rs:100-104 */
     FPG_ERR_CUDA = -100,             /* any CUDA runtime error (see fpg_last_cuda_error) */
     FPG_ERR_OUT_OF_MEMORY = -101,
     FPG_ERR_NO_DEVICE = -102
@@ -455,6 +459,119 @@ fpg_status fpg_compaction_indices_static(fpg_ctx* ctx, const uint32_t* flags_dev
 fpg_status fpg_philox_uniforms(fpg_ctx* ctx, const uint32_t key[2], const uint32_t counter[4],
                                size_t n_blocks, float* out_dev, uint32_t* out_raw_dev,
                                void* stream);
+
+/* ------------------------------------------------------------------------
+ * Convective boundary layer and convective mixing
+ * ---------------------------------------------------------------------- */
+/* HannaParams (src/pbl/mod.rs:23-57): 16 floats, 64 bytes per slot. */
+typedef struct fpg_hanna_params {
+    float ust, wst, ol, h, zeta, sigu, sigv, sigw, dsigwdz, dsigw2dz, tlu, tlv, tlw;
+    float pad[3];
+} fpg_hanna_params;
+
+/* CblSamplingInput (src/gpu/cbl.rs:38-50): uniforms in [0, 1). */
+typedef struct fpg_cbl_sampling_input {
+    float branch_uniform, gaussian_uniform0, gaussian_uniform1, pad0;
+} fpg_cbl_sampling_input;
+
+/* CblSamplingOutput (src/gpu/cbl.rs:66-92). */
+typedef struct fpg_cbl_sampling_output {
+    float sampled_w_m_s;
+    float updraft_weight, updraft_mean_m_s, updraft_sigma_m_s;
+    float downdraft_weight, downdraft_mean_m_s, downdraft_sigma_m_s;
+    float second_moment_w2, third_moment_w3, skewness, transition, z_over_h;
+} fpg_cbl_sampling_output;
+
+/* dispatch_hanna_params_gpu (src/gpu/hanna.rs:238-330, hanna_params.wgsl:
+ * 231-258): for each slot [0, dispatch_count) the PBL cell at
+ * floor(clamp(cell + pos)), 1/L -> L (hanna.rs:169-174) and
+ * compute_hanna_params (physics/hanna.rs:49-163); inactive slots get an
+ * all-zero record.  out_dev: device array of n_out records.  Errors:
+ * LengthMismatch (n_out != dispatch_count), ZeroPblShape, NotReady. */
+fpg_status fpg_dispatch_hanna_params(fpg_ctx* ctx, const fpg_particles* particles, const fpg_pbl* pbl,
+                                     fpg_hanna_params* out_dev, size_t n_out, void* stream);
+
+/* sample_cbl_vertical_velocity_gpu (src/gpu/cbl.rs:204-319, cbl.wgsl:251-298):
+ * per slot [0, dispatch_count) the CBL bi-Gaussian PDF of w' from the slot's
+ * height and Hanna record (h, w*, sigma_w, L; physics/cbl.rs:126-226) and one
+ * sample (physics/cbl.rs:274-288); inactive slots get an all-zero output.
+ * hanna_dev, inputs_dev, out_dev: device arrays.  Errors:
+ * MismatchedInputLengths (n_hanna or n_inputs != dispatch_count). */
+fpg_status fpg_cbl_sample(fpg_ctx* ctx, const fpg_particles* particles, const fpg_hanna_params* hanna_dev,
+                          size_t n_hanna, const fpg_cbl_sampling_input* inputs_dev, size_t n_inputs,
+                          fpg_cbl_sampling_output* out_dev, void* stream);
+
+/* The same sample with its inputs formed on the device: sigma_w of the Hanna
+ * parameters at the slot's PBL cell, and the first three uniforms of the
+ * Philox block at counter + slot (sample_cbl_vertical_velocity_with_rng,
+ * physics/cbl.rs:291-295, on a stream that starts at that counter).
+ * Errors: ZeroPblShape, NotReady. */
+fpg_status fpg_cbl_sample_philox(fpg_ctx* ctx, const fpg_particles* particles, const fpg_pbl* pbl,
+                                 const uint32_t key[2], const uint32_t counter[4],
+                                 fpg_cbl_sampling_output* out_dev, void* stream);
+
+/* SimplifiedEmanuelInputs (physics/convection.rs:68-82). */
+typedef struct fpg_convection_inputs {
+    const float* level_interfaces_m;        /* n_levels + 1 interfaces [m] */
+    size_t n_interfaces;
+    float convective_precip_mm_h;
+    float convective_velocity_scale_m_s;
+    float boundary_layer_height_m;
+    int32_t has_cape_override;              /* Option<f32>: 0 = None */
+    float cape_override_j_kg;
+} fpg_convection_inputs;
+
+/* The scalars of SimplifiedEmanuelColumn (physics/convection.rs:111-133) and
+ * the matrix's mixing fraction (physics/convection.rs:143-154). */
+typedef struct fpg_convection_column {
+    int32_t is_active;
+    float cape_j_kg;
+    uint32_t cloud_base_level;
+    uint32_t cloud_top_level;
+    float convective_timescale_s;
+    float mixing_fraction;
+} fpg_convection_column;
+
+/* build_simplified_convection_chain (physics/convection.rs:462-467) on the
+ * host: the column diagnostics and the column-major L*L redistribution
+ * matrix (L = n_interfaces - 1).  centers_out, mass_flux_out and
+ * detrainment_out (L floats each) may be NULL.  Errors: TooFewLevels,
+ * NonMonotonicInterfaces, InvalidBoundaryLayerHeight, InvalidTimeStep,
+ * NonStochasticColumn. */
+fpg_status fpg_convection_build_chain(const fpg_convection_inputs* inputs, float dt_seconds,
+                                      fpg_convection_column* column, float* matrix_out, float* centers_out,
+                                      float* mass_flux_out, float* detrainment_out);
+/* level_index_from_height (physics/convection.rs:469-489). */
+size_t fpg_convection_level_index(const float* level_interfaces_m, size_t n_interfaces, float height_m);
+/* apply_redistribution_matrix (physics/convection.rs:370-392) on the host:
+ * destination = M * source.  Errors: ProfileLengthMismatch. */
+fpg_status fpg_convection_apply_profile(const float* matrix_column_major, size_t level_count,
+                                        const float* source, size_t n_source, float* destination);
+
+/* A convective redistribution matrix on the device
+ * (ConvectiveRedistributionMatrix, physics/convection.rs:143-219).
+ * Errors of create: InvalidLevelCount (0 -> ZERO_SHAPE, > 65535 ->
+ * VALUE_TOO_LARGE). */
+typedef struct fpg_convection fpg_convection;
+fpg_status fpg_convection_create(fpg_ctx* ctx, size_t level_count, fpg_convection** out);
+fpg_status fpg_convection_destroy(fpg_convection* conv);
+/* Host arrays: the column-major matrix (source * L + destination, L*L
+ * floats) and the L+1 level interfaces [m].  Validates the columns as the
+ * reference's matrix type does (entries >= -1e-4 and finite, column sums
+ * within 1e-4 of 1), uploads both, and forms the expected destination height
+ * of every source level (physics/convection.rs:398-427) on the device.
+ * Returns after the upload.  Errors: LENGTH_MISMATCH (MatrixLengthMismatch /
+ * InvalidLevelInterfaces), NON_STOCHASTIC_COLUMN. */
+fpg_status fpg_convection_set_matrix(fpg_convection* conv, const float* matrix_column_major, size_t n_matrix,
+                                     const float* level_interfaces_m, size_t n_interfaces, void* stream);
+/* The expected destination heights (L floats, clamped to the column). */
+fpg_status fpg_convection_heights(const fpg_convection* conv, float* heights_host);
+/* dispatch_convective_mixing_gpu (src/gpu/convection.rs:71-250,
+ * convective_mixing.wgsl:75-113): each active slot [0, dispatch_count) moves
+ * to the expected destination height of its source level and records that
+ * level in `cbt`. */
+fpg_status fpg_convective_mixing(fpg_ctx* ctx, fpg_particles* particles, const fpg_convection* conv,
+                                 void* stream);
 
 #ifdef __cplusplus
 }

@@ -320,3 +320,260 @@ void orc_wet_cells_grid(size_t n, const float* lsp, const float* convp, const fl
         orc_wet_cell(lsp[c], convp ? convp[c] : 0.0f, cloud_cover ? cloud_cover[c] : 1.0f, a, b, &lambda_out[c],
                      &fraction_out[c]);
 }
+
+/* ---- CBL skewed vertical-velocity PDF (physics/cbl.rs) ------------------
+ * pdf[11] = updraft weight, mean, sigma; downdraft weight, mean, sigma;
+ * target w2, w3, skewness; transition; z/h.  f32 throughout, as the CPU
+ * routines run: cbrtf for f32::cbrt, powf for powf, repeated products for
+ * powi. */
+
+/* cbl_transition_factor (physics/cbl.rs:109-124). */
+float orc_cbl_transition_factor(float h, float ol) {
+    if (!isfinite(h) || h <= 0.0f || !isfinite(ol) || ol == 0.0f) return 1.0f;
+    float ratio = -h / ol;
+    float t = ratio < 15.0f ? sinf(((ratio + 10.0f) / 10.0f) * 3.14159265358979323846f) * 0.5f + 0.5f : 1.0f;
+    return fminf(fmaxf(t, 0.0f), 1.0f);
+}
+
+/* compute_cbl_moments + compute_cbl_bigaussian_pdf (physics/cbl.rs:126-226);
+ * in[5] = z, h, w*, sigma_w, L. */
+void orc_cbl_pdf(const float in[5], float pdf[11]) {
+    float h = fmaxf(in[1], 1.0f);
+    float z = fminf(fmaxf(in[0], 0.0f), h);
+    float zoh = z / h;
+    float wst = fmaxf(in[2], 0.0f);
+    float sw = fmaxf(in[3], 1.0e-5f);
+    float trans = orc_cbl_transition_factor(h, in[4]);
+    float w2 = sw * sw;
+    float shape = 1.2f * zoh * powf(1.0f - zoh, 1.5f) + 1.0e-6f;
+    float w3 = shape * (wst * wst * wst) * trans;
+    float skew = w3 / powf(w2, 1.5f);
+    float sym[11] = {0.5f, 0.0f, sw, 0.5f, 0.0f, sw, w2, w3, skew, trans, zoh};
+    memcpy(pdf, sym, sizeof(sym));
+    if (!isfinite(skew) || fabsf(skew) <= 1.0e-6f) return;
+    float fl = (2.0f / 3.0f) * cbrtf(skew);
+    float fl2 = fl * fl;
+    if (!isfinite(fl) || fabsf(fl) <= 1.0e-6f) return;
+    float skew2 = skew * skew;
+    float a1 = 1.0f + fl2, a3 = 3.0f + fl2;
+    float num = (a1 * a1 * a1) * skew2;
+    float den = (a3 * a3) * fl2;
+    float r = fmaxf(num / fmaxf(den, 1.0e-6f), 0.0f);
+    float x = sqrtf(r);
+    float aw = 0.5f * (1.0f - x / sqrtf(4.0f + r));
+    aw = fminf(fmaxf(aw, 1.0e-4f), 1.0f - 1.0e-4f);
+    float bw = 1.0f - aw;
+    float sa = sw * sqrtf(bw / (aw * (1.0f + fl2)));
+    float sb = sw * sqrtf(aw / (bw * (1.0f + fl2)));
+    pdf[0] = aw; pdf[1] = fl * sa; pdf[2] = fmaxf(sa, 1.0e-5f);
+    pdf[3] = bw; pdf[4] = -(fl * sb); pdf[5] = fmaxf(sb, 1.0e-5f);
+}
+
+/* reconstruct_cbl_moments (physics/cbl.rs:229-255): out = w2, w3, skewness. */
+void orc_cbl_reconstruct_moments(const float pdf[11], float out[3]) {
+    float wa = pdf[0], wb = pdf[3], ma = pdf[1], mb = pdf[4];
+    float s2a = pdf[2] * pdf[2], s2b = pdf[5] * pdf[5];
+    float w2 = wa * (s2a + ma * ma) + wb * (s2b + mb * mb);
+    float w3 = wa * ((ma * ma * ma) + 3.0f * ma * s2a) + wb * ((mb * mb * mb) + 3.0f * mb * s2b);
+    out[0] = w2;
+    out[1] = w3;
+    out[2] = w2 > 0.0f ? w3 / powf(w2, 1.5f) : 0.0f;
+}
+
+static float cbl_normal_pdf(float v, float mean, float sigma) {
+    sigma = fmaxf(sigma, 1.0e-5f);
+    float s = (v - mean) / sigma;
+    return (0.3989423f / sigma) * expf(-0.5f * s * s);
+}
+
+/* CblBiGaussianPdf::probability_density (physics/cbl.rs:257-270). */
+float orc_cbl_probability_density(const float pdf[11], float w) {
+    return pdf[0] * cbl_normal_pdf(w, pdf[1], pdf[2]) + pdf[3] * cbl_normal_pdf(w, pdf[4], pdf[5]);
+}
+
+/* sample_cbl_vertical_velocity (physics/cbl.rs:274-288). */
+float orc_cbl_sample(const float pdf[11], float ub, float u0, float u1) {
+    float bm[2];
+    orc_box_muller_f32(u0, u1, bm);
+    return ub < pdf[0] ? pdf[1] + pdf[2] * bm[0] : pdf[4] + pdf[5] * bm[0];
+}
+
+/* sample_cbl_vertical_velocity_with_rng (physics/cbl.rs:291-295): each call
+ * takes the four uniforms of one Philox block (next_uniform4 on a stream
+ * whose cache is empty, physics/rng.rs:130-164) and advances the counter. */
+float orc_cbl_sample_with_rng(const float pdf[11], const uint32_t key[2], uint32_t counter[4]) {
+    uint32_t b[4], next[4];
+    orc_philox4x32_10(counter, key, b);
+    orc_counter_add_u32(counter, 1u, next);
+    memcpy(counter, next, 16);
+    return orc_cbl_sample(pdf, orc_u32_to_uniform01(b[0]), orc_u32_to_uniform01(b[1]), orc_u32_to_uniform01(b[2]));
+}
+
+/* infer_cbl_branch (physics/cbl.rs:300-309): 1 updraft, 0 downdraft. */
+int32_t orc_cbl_infer_branch(float previous_w, int32_t time_direction) {
+    float sign = previous_w > 0.0f ? 1.0f : (previous_w < 0.0f ? -1.0f : (signbit(previous_w) ? -1.0f : 1.0f));
+    if (isnan(previous_w)) sign = previous_w;
+    float signed_w = sign * (time_direction >= 0 ? 1.0f : -1.0f);
+    return signed_w >= 0.0f ? 1 : 0;
+}
+
+/* sample_cbl_branch_constrained_velocity (physics/cbl.rs:315-331). */
+float orc_cbl_branch_constrained(const float pdf[11], int32_t updraft, float u0, float u1, int32_t time_direction) {
+    float bm[2];
+    orc_box_muller_f32(u0, u1, bm);
+    float eta = bm[0];
+    float speed = updraft ? fabsf(pdf[1] + pdf[2] * eta) : -(fabsf(pdf[4]) + pdf[5] * fabsf(eta));
+    return speed * (time_direction >= 0 ? 1.0f : -1.0f);
+}
+
+/* The dispatch of src/gpu/cbl.rs (cbl.wgsl:251-298) over n slots: hanna16 is
+ * HannaParams records (h at [3], w* at [1], L at [2], sigma_w at [7]), in4
+ * the sampling inputs; out12 = sample, pdf[11]; zeros for inactive slots. */
+void orc_cbl_sample_slots(size_t n, const uint32_t* flags, const float* pos_z, const float* hanna16,
+                          const float* in4, float* out12) {
+    for (size_t p = 0; p < n; ++p) {
+        float* o = out12 + 12 * p;
+        if (!(flags[p] & 1u)) { memset(o, 0, 12 * sizeof(float)); continue; }
+        const float* hp = hanna16 + 16 * p;
+        float in[5] = {pos_z[p], hp[3], hp[1], hp[7], hp[2]};
+        float pdf[11];
+        orc_cbl_pdf(in, pdf);
+        o[0] = orc_cbl_sample(pdf, in4[4 * p], in4[4 * p + 1], in4[4 * p + 2]);
+        memcpy(o + 1, pdf, sizeof(pdf));
+    }
+}
+
+/* compute_hanna_params_gpu (hanna_params.wgsl:231-258) over n slots with
+ * compute_hanna_params_from_pbl (physics/hanna.rs:178-194); out16 records,
+ * zeros for inactive slots. */
+void orc_hanna_params_slots(size_t n, const int32_t* cell_x, const int32_t* cell_y, const float* pos_x,
+                            const float* pos_y, const float* pos_z, const uint32_t* flags, const float* ustar,
+                            const float* wstar, const float* hmix, const float* oli, size_t pnx, size_t pny,
+                            float* out16) {
+    for (size_t p = 0; p < n; ++p) {
+        float* o = out16 + 16 * p;
+        memset(o, 0, 16 * sizeof(float));
+        if (!(flags[p] & 1u)) continue;
+        float x = (float)cell_x[p] + pos_x[p];
+        float y = (float)cell_y[p] + pos_y[p];
+        size_t i = (size_t)floorf(fminf(fmaxf(x, 0.0f), (float)(pnx - 1)));
+        size_t j = (size_t)floorf(fminf(fmaxf(y, 0.0f), (float)(pny - 1)));
+        size_t c = i * pny + j;
+        orc_hanna_f32(ustar[c], wstar[c], orc_obukhov_from_inverse_f32(oli[c]), hmix[c], pos_z[p], o);
+    }
+}
+
+/* ---- Convection chain (physics/convection.rs) --------------------------- */
+
+/* level_index_from_height (physics/convection.rs:469-489). */
+size_t orc_level_index_from_height(const float* iface, size_t n_iface, float height) {
+    size_t L = n_iface > 0 ? n_iface - 1 : 0;
+    if (L == 0) return 0;
+    float z = fminf(fmaxf(height, iface[0]), iface[L]);
+    for (size_t l = 0; l < L; ++l)
+        if (z >= iface[l] && z < iface[l + 1]) return l;
+    return L - 1;
+}
+
+/* build_simplified_convection_chain (physics/convection.rs:222-367, 462-467).
+ * info[6] = is_active, cape, cloud base, cloud top, timescale, mixing
+ * fraction.  Returns 0 or the FPG_ERR_* of the reference error. */
+int32_t orc_convection_chain(const float* iface, size_t n_iface, float precip, float wstar_in, float hbl,
+                             int32_t has_cape, float cape_override, float dt, float* matrix, float* det_out,
+                             float* info) {
+    if (n_iface < 2) return FPG_ERR_TOO_FEW_LEVELS;
+    for (size_t i = 0; i + 1 < n_iface; ++i)
+        if (!isfinite(iface[i]) || !isfinite(iface[i + 1]) || iface[i + 1] <= iface[i])
+            return FPG_ERR_NON_MONOTONIC_INTERFACES;
+    if (!isfinite(hbl) || hbl < 0.0f) return FPG_ERR_INVALID_BOUNDARY_LAYER_HEIGHT;
+    size_t L = n_iface - 1;
+    float cape;
+    if (has_cape) {
+        cape = cape_override;
+    } else {
+        float w = fmaxf(wstar_in, 0.0f);
+        cape = 350.0f * w * w + 35.0f * fmaxf(precip, 0.0f);
+    }
+    int active = cape >= 5.0f && precip >= 0.05f;
+    float* det = calloc(L, sizeof(float));
+    size_t base = 0, top = 0;
+    float timescale = 3600.0f;
+    if (active) {
+        float ctop = iface[L];
+        float base_h = fminf(fmaxf(0.6f * hbl, iface[0]), ctop);
+        base = orc_level_index_from_height(iface, n_iface, base_h);
+        float depth = 1500.0f + 20.0f * sqrtf(cape);
+        float top_h = fminf(fmaxf(base_h + depth, base_h), ctop);
+        top = orc_level_index_from_height(iface, n_iface, top_h);
+        if (top < base) top = base;
+        size_t span = top - base;
+        float peak = 0.02f * sqrtf(cape) * (1.0f + 0.1f * fmaxf(precip, 0.0f));
+        float sum = 0.0f;
+        for (size_t l = base; l <= top; ++l) {
+            float nrm = span == 0 ? 0.5f : (float)(l - base) / (float)span;
+            float bell = fmaxf(4.0f * nrm * (1.0f - nrm), 0.0f);
+            float f = peak * (0.05f + bell);
+            det[l] = f;
+            sum += f;
+        }
+        if (sum > 0.0f) {
+            for (size_t l = 0; l < L; ++l) det[l] /= sum;
+        } else {
+            for (size_t l = base; l <= top; ++l) det[l] = 1.0f / (float)(top - base + 1);
+        }
+        float intensity = fminf(fmaxf(cape / 1200.0f + fmaxf(precip, 0.0f) / 20.0f, 0.0f), 1.0f);
+        timescale = 3600.0f - intensity * (3600.0f - 300.0f);
+    }
+    if (!isfinite(dt) || dt <= 0.0f) { free(det); return FPG_ERR_INVALID_TIME_STEP; }
+    memset(matrix, 0, L * L * sizeof(float));
+    for (size_t l = 0; l < L; ++l) matrix[l * L + l] = 1.0f;
+    float mixing = 0.0f;
+    if (active) {
+        float ts = fminf(fmaxf(timescale, 300.0f), 3600.0f);
+        float cf = fminf(fmaxf(cape / (cape + 100.0f), 0.0f), 1.0f);
+        mixing = fminf(fmaxf((1.0f - expf(-dt / ts)) * cf, 0.0f), 0.95f);
+        for (size_t s = base; s <= top; ++s)
+            for (size_t d = 0; d < L; ++d) {
+                float v = mixing * det[d];
+                if (d == s) v += 1.0f - mixing;
+                matrix[s * L + d] = v;
+            }
+    }
+    if (det_out) memcpy(det_out, det, L * sizeof(float));
+    free(det);
+    info[0] = (float)active;
+    info[1] = active ? cape : fmaxf(cape, 0.0f);
+    info[2] = (float)base;
+    info[3] = (float)top;
+    info[4] = timescale;
+    info[5] = mixing;
+    return FPG_OK;
+}
+
+/* apply_convective_mixing_to_particles_cpu (physics/convection.rs:431-459)
+ * with expected_destination_height_m (physics/convection.rs:398-427). */
+void orc_convective_mixing(size_t n, const uint32_t* flags, float* pos_z, int32_t* cbt, const float* matrix,
+                           size_t L, const float* iface, const float* centers) {
+    float zmin = iface[0], zmax = iface[L];
+    for (size_t p = 0; p < n; ++p) {
+        if (!(flags[p] & 1u)) continue;
+        size_t s = orc_level_index_from_height(iface, L + 1, pos_z[p]);
+        float wh = 0.0f, sum = 0.0f;
+        for (size_t d = 0; d < L; ++d) {
+            float w = fmaxf(matrix[s * L + d], 0.0f);
+            wh += w * centers[d];
+            sum += w;
+        }
+        float dest = sum > 0.0f ? wh / sum : centers[s];
+        pos_z[p] = fminf(fmaxf(dest, zmin), zmax);
+        cbt[p] = (int32_t)s;
+    }
+}
+
+/* n successive sample_cbl_vertical_velocity_with_rng calls on one stream. */
+void orc_cbl_sample_stream(const float pdf[11], const uint32_t key[2], const uint32_t counter[4], size_t n,
+                           float* out) {
+    uint32_t c[4];
+    memcpy(c, counter, 16);
+    for (size_t i = 0; i < n; ++i) out[i] = orc_cbl_sample_with_rng(pdf, key, c);
+}

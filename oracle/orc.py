@@ -487,3 +487,139 @@ def geo_to_relative(lon, lat, domain):
     st = lib.orc_geo_to_relative(ctypes.c_double(lon), ctypes.c_double(lat), d, ctypes.byref(cx),
                                  ctypes.byref(cy), ctypes.byref(fx), ctypes.byref(fy))
     return st, cx.value, cy.value, fx.value, fy.value
+
+
+# ---- CBL skewed PDF and convective mixing (physics/cbl.rs, physics/convection.rs)
+
+CBL_PDF_FIELDS = ["updraft_weight", "updraft_mean_m_s", "updraft_sigma_m_s", "downdraft_weight",
+                  "downdraft_mean_m_s", "downdraft_sigma_m_s", "second_moment_w2", "third_moment_w3", "skewness",
+                  "transition", "z_over_h"]
+
+lib.orc_cbl_transition_factor.restype = ctypes.c_float
+lib.orc_cbl_transition_factor.argtypes = [ctypes.c_float, ctypes.c_float]
+lib.orc_cbl_probability_density.restype = ctypes.c_float
+lib.orc_cbl_probability_density.argtypes = [_f32p, ctypes.c_float]
+lib.orc_cbl_sample.restype = ctypes.c_float
+lib.orc_cbl_sample.argtypes = [_f32p, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+lib.orc_cbl_branch_constrained.restype = ctypes.c_float
+lib.orc_cbl_branch_constrained.argtypes = [_f32p, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32]
+lib.orc_cbl_infer_branch.restype = ctypes.c_int32
+lib.orc_cbl_infer_branch.argtypes = [ctypes.c_float, ctypes.c_int32]
+lib.orc_level_index_from_height.restype = ctypes.c_size_t
+lib.orc_level_index_from_height.argtypes = [_f32p, ctypes.c_size_t, ctypes.c_float]
+lib.orc_convection_chain.restype = ctypes.c_int32
+lib.orc_convection_chain.argtypes = [_f32p, ctypes.c_size_t, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_int32, ctypes.c_float, ctypes.c_float, _f32p, _f32p, _f32p]
+
+
+def cbl_transition_factor(h, ol):
+    return lib.orc_cbl_transition_factor(h, ol)
+
+
+def cbl_pdf(z, h, wstar, sigma_w, ol) -> np.ndarray:
+    """compute_cbl_bigaussian_pdf: the 11 floats of CBL_PDF_FIELDS."""
+    inp = np.array([z, h, wstar, sigma_w, ol], np.float32)
+    out = np.zeros(11, np.float32)
+    lib.orc_cbl_pdf(_ptr(inp), _ptr(out))
+    return out
+
+
+def cbl_reconstruct_moments(pdf) -> np.ndarray:
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    out = np.zeros(3, np.float32)
+    lib.orc_cbl_reconstruct_moments(_ptr(pdf), _ptr(out))
+    return out
+
+
+def cbl_probability_density(pdf, w) -> float:
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    return lib.orc_cbl_probability_density(_ptr(pdf, _f32p), w)
+
+
+def cbl_sample(pdf, branch_uniform, u0, u1) -> float:
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    return lib.orc_cbl_sample(_ptr(pdf, _f32p), branch_uniform, u0, u1)
+
+
+def cbl_sample_stream(pdf, key, counter, n) -> np.ndarray:
+    """n successive sample_cbl_vertical_velocity_with_rng draws."""
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    k = np.array(key, np.uint32)
+    c = np.array(counter, np.uint32)
+    out = np.zeros(n, np.float32)
+    lib.orc_cbl_sample_stream(_ptr(pdf), _ptr(k), _ptr(c), ctypes.c_size_t(n), _ptr(out))
+    return out
+
+
+def cbl_infer_branch(previous_w, time_direction) -> str:
+    return "updraft" if lib.orc_cbl_infer_branch(previous_w, time_direction) else "downdraft"
+
+
+def cbl_branch_constrained(pdf, branch, u0, u1, time_direction) -> float:
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    return lib.orc_cbl_branch_constrained(_ptr(pdf, _f32p), 1 if branch == "updraft" else 0, u0, u1, time_direction)
+
+
+def cbl_sample_slots(rec, hanna16, inputs) -> np.ndarray:
+    """The CBL dispatch over records: (n, 12) = sample + PDF, zeros inactive."""
+    n = rec.size
+    flags = np.ascontiguousarray(rec["flags"], np.uint32)
+    z = np.ascontiguousarray(rec["pos_z"], np.float32)
+    h = np.ascontiguousarray(hanna16.view(np.float32).reshape(n, 16) if hanna16.dtype.names else hanna16,
+                             np.float32)
+    i4 = np.ascontiguousarray(inputs.view(np.float32).reshape(n, 4) if inputs.dtype.names else inputs, np.float32)
+    out = np.zeros((max(n, 1), 12), np.float32)
+    lib.orc_cbl_sample_slots(ctypes.c_size_t(n), _ptr(flags), _ptr(z), _ptr(h), _ptr(i4), _ptr(out))
+    return out[:n]
+
+
+def hanna_params_slots(rec, ustar, wstar, hmix, oli, pnx, pny) -> np.ndarray:
+    """compute_hanna_params_gpu over records: (n, 16) HannaParams floats."""
+    n = rec.size
+    cols = {k: np.ascontiguousarray(rec[k]) for k in ("cell_x", "cell_y", "pos_x", "pos_y", "pos_z", "flags")}
+    f = [np.ascontiguousarray(a, np.float32).reshape(-1) for a in (ustar, wstar, hmix, oli)]
+    out = np.zeros((max(n, 1), 16), np.float32)
+    lib.orc_hanna_params_slots(ctypes.c_size_t(n), _ptr(cols["cell_x"]), _ptr(cols["cell_y"]), _ptr(cols["pos_x"]),
+                               _ptr(cols["pos_y"]), _ptr(cols["pos_z"]), _ptr(cols["flags"]), _ptr(f[0]),
+                               _ptr(f[1]), _ptr(f[2]), _ptr(f[3]), ctypes.c_size_t(pnx), ctypes.c_size_t(pny),
+                               _ptr(out))
+    return out[:n]
+
+
+def level_index_from_height(iface, height) -> int:
+    iface = np.ascontiguousarray(iface, np.float32)
+    return int(lib.orc_level_index_from_height(_ptr(iface, _f32p), iface.size, height))
+
+
+def convection_chain(iface, precip, wstar, hbl, cape_override, dt):
+    """(status, matrix (L, L) column-major as [source, destination],
+    detrainment weights, info dict)."""
+    iface = np.ascontiguousarray(iface, np.float32)
+    L = max(iface.size - 1, 1)
+    m = np.zeros(L * L, np.float32)
+    det = np.zeros(L, np.float32)
+    info = np.zeros(6, np.float32)
+    st = lib.orc_convection_chain(_ptr(iface, _f32p), iface.size, precip, wstar, hbl,
+                                  0 if cape_override is None else 1,
+                                  0.0 if cape_override is None else cape_override, dt, _ptr(m, _f32p),
+                                  _ptr(det, _f32p), _ptr(info, _f32p))
+    keys = ["is_active", "cape_j_kg", "cloud_base_level", "cloud_top_level", "convective_timescale_s",
+            "mixing_fraction"]
+    return st, m, det, dict(zip(keys, info.tolist()))
+
+
+def convective_mixing(rec, matrix, iface):
+    """apply_convective_mixing_to_particles_cpu on a copy of the records."""
+    out = rec.copy()
+    iface = np.ascontiguousarray(iface, np.float32)
+    L = iface.size - 1
+    centers = (np.float32(0.5) * (iface[:-1] + iface[1:])).astype(np.float32)
+    flags = np.ascontiguousarray(out["flags"])
+    z = np.ascontiguousarray(out["pos_z"])
+    cbt = np.ascontiguousarray(out["cbt"])
+    m = np.ascontiguousarray(matrix, np.float32)
+    lib.orc_convective_mixing(ctypes.c_size_t(out.size), _ptr(flags), _ptr(z), _ptr(cbt), _ptr(m),
+                              ctypes.c_size_t(L), _ptr(iface), _ptr(centers))
+    out["pos_z"] = z
+    out["cbt"] = cbt
+    return out

@@ -60,12 +60,20 @@ def test_record_layouts_match_the_c_header(tmp_path):
         "fpg_receptor_release": R.ReceptorRelease, "fpg_source_region": R.SourceRegion,
         "fpg_source_collection": R.SourceCollection, "fpg_backward_config": R.BackwardConfig,
         "fpg_inverse_config": R.InverseConfig,
-        "fpg_batch_config": R.BatchConfig,
+        "fpg_batch_config": R.BatchConfig, "fpg_convection_inputs": R.ConvectionInputs,
+        "fpg_convection_column": R.ConvectionColumn,
     }
+    dtypes = {"fpg_hanna_params": R.HANNA_PARAMS_DTYPE, "fpg_cbl_sampling_input": R.CBL_INPUT_DTYPE,
+              "fpg_cbl_sampling_output": R.CBL_OUTPUT_DTYPE, "fpg_particle": R.PARTICLE_DTYPE,
+              "fpg_surface_cell": R.SURFACE_DTYPE}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fpg_adjoint.h"', "int main(void) {"]
     for c, py in pairs.items():
         lines.append(f'printf("{c} size %zu\\n", sizeof({c}));')
         for name, _ in py._fields_:
+            lines.append(f'printf("{c} {name} %zu\\n", offsetof({c}, {name}));')
+    for c, dt in dtypes.items():
+        lines.append(f'printf("{c} size %zu\\n", sizeof({c}));')
+        for name in dt.names:
             lines.append(f'printf("{c} {name} %zu\\n", offsetof({c}, {name}));')
     lines.append("return 0; }")
     src = tmp_path / "layout.c"
@@ -81,6 +89,10 @@ def test_record_layouts_match_the_c_header(tmp_path):
         assert got[(c, "size")] == ctypes.sizeof(py), c
         for name, _ in py._fields_:
             assert got[(c, name)] == getattr(py, name).offset, (c, name)
+    for c, dt in dtypes.items():
+        assert got[(c, "size")] == dt.itemsize, c
+        for name in dt.names:
+            assert got[(c, name)] == dt.fields[name][1], (c, name)
 
 
 def test_batch_tuning_candidates_listed_without_a_device():
