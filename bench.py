@@ -76,6 +76,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-scenarios", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-cbl", action="store_true", help="skip the CBL / convective-mixing kernel timings")
     ap.add_argument("--sort-every", type=int, default=SORT_EVERY,
                     help="steps between spatial reorders of the population")
     ap.add_argument("--adjoint-instances", type=int, default=64)
@@ -470,6 +471,79 @@ def run_adjoint(ctx, stream, args, rank, world):
     return out
 
 
+def run_cbl_convection(ctx, stream, parts, pbl, n_active, peak, args, rank, world):
+    """The CBL and convective-mixing kernels over the spun-up population of
+    the global run (every slot of the dispatch, n_active of them active),
+    each launch timed alone with CUDA events after an L2 flush (a 256 MB
+    write), 3 warm-up launches, then 10 timed.  Algorithmic bytes per slot:
+    convective mixing 16 (flags + pos_z read, pos_z + cbt written; 4 for an
+    inactive slot), fused CBL sampler 72 (flags, cell_x/y, pos_x/y/z read;
+    the 48-byte output written), Hanna records 88 (the same 24 read, 64
+    written), record-form CBL sampler 92 (flags, pos_z, 20 bytes of the
+    Hanna record, 16 of uniforms read; 48 written).  Per-cell PBL gathers
+    (1 MB, L2-resident) are not counted."""
+    import torch
+
+    from flexpart_gpu import cbl
+    from flexpart_gpu import convection as cv
+    from flexpart_gpu.records import CBL_INPUT_DTYPE, CBL_OUTPUT_DTYPE
+
+    n = parts.dispatch_count
+    flush = torch.empty(64 * 2**20, dtype=torch.int32, device="cuda")
+
+    def per_launch_ms(fn, reps=10):
+        for _ in range(3):
+            fn()
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            ctx.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+
+    def entry(ms, bytes_):
+        gbs = bytes_ / (ms / 1e3) / 1e9
+        return {"ms": ms, "algorithmic_bytes": bytes_, "achieved_gbs": gbs, "frac": gbs / peak}
+
+    out = {"slots": n, "active": n_active}
+    hanna = api_device(ctx, n, cbl.HANNA_PARAMS_DTYPE)
+    out_rec = api_device(ctx, n, CBL_OUTPUT_DTYPE)
+    rng = np.random.default_rng(17 + rank)
+    u = np.zeros(n, CBL_INPUT_DTYPE)
+    u["branch_uniform"], u["gaussian_uniform0"], u["gaussian_uniform1"] = (rng.random(n, np.float32)
+                                                                             for _ in range(3))
+    inputs = api_device(ctx, n, CBL_INPUT_DTYPE)
+    inputs.upload(u)
+    del u
+    ms = per_launch_ms(lambda: cbl.dispatch_hanna_params_gpu(ctx, parts, pbl, hanna))
+    out["hanna_params"] = entry(ms, 88 * n_active + 68 * (n - n_active))
+    ms = per_launch_ms(lambda: cbl.sample_cbl_vertical_velocity_philox(ctx, parts, pbl, (1, 2), (3, 0, 0, 0),
+                                                                       out_rec))
+    out["cbl_sample_philox"] = entry(ms, 72 * n_active + 52 * (n - n_active))
+    ms = per_launch_ms(lambda: cbl.sample_cbl_vertical_velocity_gpu(ctx, parts, hanna, inputs, out_rec))
+    out["cbl_sample_records"] = entry(ms, 92 * n_active + 52 * (n - n_active))
+    del hanna, out_rec, inputs
+    iface = [0.0, 400.0, 1000.0, 2000.0, 3500.0, 5000.0, 7000.0, 9000.0, 12000.0, 16000.0, 20000.0]
+    _, matrix = cv.build_simplified_convection_chain(cv.SimplifiedEmanuelInputs(iface, 10.0, 2.5, 900.0), 900.0)
+    mix = cv.ConvectiveMixing(ctx, matrix.level_count())
+    mix.set_matrix(matrix, iface)
+    ms = per_launch_ms(lambda: mix.apply(parts))
+    out["convective_mixing"] = entry(ms, 16 * n_active + 4 * (n - n_active))
+    out["convective_mixing"]["levels"] = matrix.level_count()
+    out["l2"] = "256 MB write between timed launches"
+    return out
+
+
+def api_device(ctx, n, dtype):
+    from flexpart_gpu import api
+    return api.DeviceArray(ctx, n, dtype)
+
+
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
@@ -558,6 +632,19 @@ def main():
     # torch's collectives run on its current stream: make that the library's stream
     torch.cuda.set_stream(stream)
 
+    stage_ev = {"reorder": [], "pbl": [], "grid": []}
+
+    def staged(name, record, fn):
+        if not record:
+            return fn()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        stage_ev[name].append((a, b))
+        return r
+
     def one_step(record: bool):
         t = state["t"]
         fa, fb, ta, tb = synthetic.bracket_frames(scn, t)
@@ -566,8 +653,8 @@ def main():
             state["bracket"] = (fa, fb, ta)
         alpha = (t - ta) / float(tb - ta)
         if state["k"] % args.sort_every == 0:
-            sorter.sort(parts, met)
-        api.pbl_diagnostics(ctx, surf, alpha, pbl)
+            staged("reorder", record, lambda: sorter.sort(parts, met))
+        staged("pbl", record, lambda: api.pbl_diagnostics(ctx, surf, alpha, pbl))
         prm = StepParams.production(alpha=alpha, dt_seconds=float(scn.dt), turb_dt_seconds=float(scn.dt),
                                     x_grid_per_meter=xs, y_grid_per_meter=ys, z_grid_per_meter=zs, key=scn.key,
                                     counter=state["counter"], dry_mode=1, dry_velocity_m_s=scn.dry_velocity,
@@ -581,7 +668,7 @@ def main():
             b.record(stream)
             ev.append((a, b))
         if state["k"] % 12 == 11:
-            grid.accumulate(parts, 0, 1e6, scn.outheights)
+            staged("grid", record, lambda: grid.accumulate(parts, 0, 1e6, scn.outheights))
             if world > 1:
                 # the one exchange: the ranks' integer grids summed (mod 2^32) over NCCL
                 fd.allreduce_grids_device(lib.fpg_grid_counts_device(grid.h), lib.fpg_grid_mass_device(grid.h),
@@ -616,6 +703,11 @@ def main():
         elapsed_ms = float(tt.item())
     kernel_ms = [a.elapsed_time(b) for a, b in ev]
     avg_kernel_ms = sum(kernel_ms) / len(kernel_ms)
+    stages = {"step_kernel_ms": avg_kernel_ms}
+    for name, evs in stage_ev.items():
+        if evs:
+            stages[f"{name}_ms"] = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+            stages[f"{name}_per_window"] = len(evs)
     value = n_active * args.steps * world / (elapsed_ms / 1e3)
     peak, peak_kind = measured_peak_hbm()
     achieved = BYTES_PER_PARTICLE_STEP * n_active / (avg_kernel_ms / 1e3) / 1e9
@@ -640,6 +732,7 @@ def main():
             pinned.append(pf)
         drv.enable_met_ring(3)
         fs = spec.frame_seconds
+        copy_stream = torch.cuda.Stream()
 
         def prefetch(tf):
             if tf in seen["prefetched"]:
@@ -663,8 +756,8 @@ def main():
             prefetch(tb + fs)       # the next bracket's new frame, while this one is in use
             api.check(lib.fpg_forward_accumulate_grid(drv.h, grid.h, 0, 1e6, ctypes.c_void_p(oh.ctypes.data),
                                                       oh.size), "grid")
-            api.check(lib.fpg_grid_download(grid.h, ctypes.c_void_p(counts_h.data_ptr()),
-                                            ctypes.c_void_p(mass_h.data_ptr()), None, None), "grid download")
+            # the step's grid to pinned host memory on the copy stream, under the next step's compute
+            grid.download_async(counts_h.data_ptr(), mass_h.data_ptr(), ctypes.c_void_p(copy_stream.cuda_stream))
 
         for _ in range(args.warmup):
             e2e_step()
@@ -680,6 +773,7 @@ def main():
         a.record(stream)
         for _ in range(args.steps):
             e2e_step()
+        stream.wait_stream(copy_stream)            # the last grid is on the host inside the timed region
         b.record(stream)
         ctx.synchronize()
         ms = a.elapsed_time(b)
@@ -693,7 +787,8 @@ def main():
                "met_ring": dict(zip(("bracket_hits", "host_uploads"),
                                     (a1 - a0 for a1, a0 in zip(drv.met_ring_stats(), ring0)))),
                "path": "fpg_forward_prefetch_frame (met frames from pinned host memory, one bracket ahead) + "
-                       "fpg_forward_run_timestep + fpg_forward_accumulate_grid + fpg_grid_download"}
+                       "fpg_forward_run_timestep + fpg_forward_accumulate_grid + fpg_grid_download_async "
+                       "(every step's grid to pinned host memory on a copy stream)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -711,6 +806,9 @@ def main():
     adjoint = None
     if not args.no_adjoint and not args.quick:
         adjoint = run_adjoint(ctx, stream, args, rank, world)
+    cbl_conv = None
+    if not args.no_cbl:
+        cbl_conv = run_cbl_convection(ctx, stream, parts, pbl, n_active, peak, args, rank, world)
 
     if rank == 0:
         line = {
@@ -729,12 +827,14 @@ def main():
                          "peak_kind": peak_kind,
                          "kernel": "fused_step_kernel", "kernel_ms": avg_kernel_ms,
                          "bytes_per_launch": BYTES_PER_PARTICLE_STEP * n_active},
+            "stages": stages,
             "clocks": clk,
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,
+            "cbl_convection": cbl_conv,
         }
         print(json.dumps(line), flush=True)
     del drv

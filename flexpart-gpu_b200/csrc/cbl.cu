@@ -13,7 +13,7 @@
 //   once per level when the matrix is set (one thread per level, the same
 //   sequential f32 sum the reference runs per particle); the per-particle
 //   kernel is a level search plus one table read: 8 bytes read and 8 bytes
-//   written per active slot, HBM-bound.
+//   written per active slot, four slots per thread, HBM-bound.
 //
 // The PDF follows the CPU routine (physics/cbl.rs:126-226): cbrt for the
 // signed cube root and repeated multiplication for powi(3) / powi(2); the
@@ -221,31 +221,56 @@ __global__ void conv_heights_kernel(uint32_t L, const float* __restrict__ m, con
 // lower <= z < upper, else the top level) is the last level whose lower
 // interface is <= z, found by bisection; otherwise the scan itself runs.
 template <bool kSorted>
-__global__ void __launch_bounds__(256) conv_apply_kernel(size_t n, const uint32_t* __restrict__ flags,
-                                                         float* __restrict__ pos_z, int32_t* __restrict__ cbt,
-                                                         uint32_t L, const float* __restrict__ iface,
-                                                         const float* __restrict__ heights,
-                                                         const uint32_t* __restrict__ has_weight) {
-    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    if ((flags[p] & FLAG_ACTIVE) == 0u) return;
-    const float z_min = __ldg(iface), z_max = __ldg(iface + L);
-    const float z = clampf(pos_z[p], z_min, z_max);
-    uint32_t level = L - 1u;
+__device__ __forceinline__ uint32_t source_level(float z, uint32_t L, const float* __restrict__ iface) {
     if constexpr (kSorted) {
         uint32_t lo = 0u, hi = L;                 // count of iface[0..L) <= z lies in [1, L]
         while (hi - lo > 1u) {
             const uint32_t mid = (lo + hi) >> 1;
             if (__ldg(iface + mid) <= z) lo = mid; else hi = mid;
         }
-        level = lo;
+        return lo;
     } else {
-        for (uint32_t l = 0; l < L; ++l) {
-            if (z >= __ldg(iface + l) && z < __ldg(iface + l + 1u)) { level = l; break; }
-        }
+        for (uint32_t l = 0; l < L; ++l)
+            if (z >= __ldg(iface + l) && z < __ldg(iface + l + 1u)) return l;
+        return L - 1u;
     }
+}
+
+template <bool kSorted>
+__device__ __forceinline__ void mix_slot(size_t p, float z_in, float* __restrict__ pos_z, int32_t* __restrict__ cbt,
+                                         uint32_t L, const float* __restrict__ iface,
+                                         const float* __restrict__ heights, const uint32_t* __restrict__ has_weight,
+                                         float z_min, float z_max) {
+    const float z = clampf(z_in, z_min, z_max);
+    const uint32_t level = source_level<kSorted>(z, L, iface);
     pos_z[p] = __ldg(has_weight + level) ? __ldg(heights + level) : z;
     cbt[p] = (int32_t)level;
+}
+
+// Four slots per thread: the flags and heights of a quad arrive in one
+// 16-byte load each (the fields are 256-byte aligned); only active slots
+// are written.  The last n % 4 slots take scalar loads.
+template <bool kSorted>
+__global__ void __launch_bounds__(256) conv_apply_kernel(size_t n, const uint32_t* __restrict__ flags,
+                                                         float* __restrict__ pos_z, int32_t* __restrict__ cbt,
+                                                         uint32_t L, const float* __restrict__ iface,
+                                                         const float* __restrict__ heights,
+                                                         const uint32_t* __restrict__ has_weight) {
+    const size_t p0 = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 4u;
+    if (p0 >= n) return;
+    const float z_min = __ldg(iface), z_max = __ldg(iface + L);
+    if (p0 + 4u <= n) {
+        const uint4 f = __ldg(reinterpret_cast<const uint4*>(flags + p0));
+        const float4 z = *reinterpret_cast<const float4*>(pos_z + p0);
+        if (f.x & FLAG_ACTIVE) mix_slot<kSorted>(p0, z.x, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
+        if (f.y & FLAG_ACTIVE) mix_slot<kSorted>(p0 + 1, z.y, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
+        if (f.z & FLAG_ACTIVE) mix_slot<kSorted>(p0 + 2, z.z, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
+        if (f.w & FLAG_ACTIVE) mix_slot<kSorted>(p0 + 3, z.w, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
+    } else {
+        for (size_t p = p0; p < n; ++p)
+            if (flags[p] & FLAG_ACTIVE)
+                mix_slot<kSorted>(p, pos_z[p], pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
+    }
 }
 
 }  // namespace
@@ -411,7 +436,7 @@ extern "C" fpg_status fpg_convective_mixing(fpg_ctx* ctx, fpg_particles* P, cons
     const auto* flags = static_cast<const uint32_t*>(P->field[FPG_FIELD_FLAGS]);
     auto* pos_z = static_cast<float*>(P->field[FPG_FIELD_POS_Z]);
     auto* cbt = static_cast<int32_t*>(P->field[FPG_FIELD_CBT]);
-    const unsigned grid = (unsigned)((n + 255) / 256);
+    const unsigned grid = (unsigned)(((n + 3) / 4 + 255) / 256);
     if (c->sorted)
         conv_apply_kernel<true><<<grid, 256, 0, ctx->pick(stream)>>>(n, flags, pos_z, cbt, (uint32_t)c->levels,
                                                                     c->iface, c->heights, c->has_weight);

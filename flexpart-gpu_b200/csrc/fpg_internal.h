@@ -89,6 +89,12 @@ struct fpg_grid {
     uint32_t* counts = nullptr;
     uint32_t* mass = nullptr;
     float mass_scale = 1.0e6f;
+    // fpg_grid_download_async: the copy waits for `produced` (recorded on the
+    // stream of the last accumulate); the next accumulate waits for `copied`.
+    cudaStream_t last_stream = nullptr;
+    cudaEvent_t produced = nullptr;
+    cudaEvent_t copied = nullptr;
+    bool copy_pending = false;
 };
 
 struct fpg_compaction {

@@ -3,13 +3,15 @@
 //
 // Each active particle adds 1 to its cell's count and u32(mass*scale+0.5) to
 // its cell's scaled mass.  Both grids are u32 sums, so the result is the same
-// whatever order the additions happen in.  A warp first merges the particles
-// that share a cell (one __match-style pass per distinct cell in the warp,
-// __reduce_add_sync of the scaled masses) and issues one pair of atomics per
-// distinct cell instead of one per particle; particles released together
-// stay close together, so a warp usually holds very few distinct cells.
+// whatever order the additions happen in.  Plumes put ~1e5 particles in a
+// cell, so one global atomic per particle (or per warp) serialises on the
+// hot cells: a warp first merges the particles that share a cell, a CTA
+// merges its warps' sums in a shared-memory table over one contiguous chunk
+// of slots, and the grid receives one pair of atomics per distinct cell per
+// CTA.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -35,33 +37,98 @@ __device__ __forceinline__ uint32_t cell_of(const GridArgs& a, const float* h, u
     return (ix * a.ny + iy) * a.nz + iz;
 }
 
-__global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, uint32_t* __restrict__ counts,
-                                                   uint32_t* __restrict__ mass) {
-    __shared__ float s_h[FPG_MAX_LEVELS];
-    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_h[i] = lt.h[i];
-    __syncthreads();
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned lane = threadIdx.x & 31u;
-    bool valid = false;
-    uint32_t key = 0xffffffffu, q = 0u;
-    if (p < a.n && (a.flags[p] & 1u)) {
-        valid = true;
-        key = cell_of(a, s_h, p);
-        q = quantize(fmaxf(a.mass[p], 0.0f), a.mass_scale);
-    }
-    // warp-uniform loop over the distinct cells held by this warp
-    unsigned pending = __ballot_sync(0xffffffffu, valid);
-    while (pending) {
-        const int src = __ffs(pending) - 1;
-        const uint32_t k = __shfl_sync(0xffffffffu, key, src);
-        const bool mine = valid && key == k;
-        const unsigned grp = __ballot_sync(0xffffffffu, mine);
-        const uint32_t qs = __reduce_add_sync(0xffffffffu, mine ? q : 0u);
-        if (lane == (unsigned)src) {
-            atomicAdd(counts + k, (uint32_t)__popc(grp));
-            atomicAdd(mass + k, qs);
+// The CTA's table of the cells its chunk touches: open addressing on the
+// cell index in shared memory, filled with shared atomics and added to the
+// global grid at the end, one pair of atomics per distinct cell per CTA.
+constexpr uint32_t kTableBits = 10;
+constexpr uint32_t kTable = 1u << kTableBits;             // 1024 entries
+constexpr uint32_t kProbes = 8;
+constexpr uint32_t kEmpty = 0xffffffffu;   // no cell has this index (cells < 2^32 - 1)
+
+__device__ __forceinline__ void table_add(uint32_t* tk, uint32_t* tc, uint32_t* tm, uint32_t k, uint32_t c,
+                                          uint32_t m, uint32_t* __restrict__ counts, uint32_t* __restrict__ mass) {
+    uint32_t slot = (k * 2654435761u) >> (32 - kTableBits);
+    for (uint32_t i = 0; i < kProbes; ++i) {
+        const uint32_t old = atomicCAS(tk + slot, kEmpty, k);
+        if (old == kEmpty || old == k) {
+            atomicAdd(tc + slot, c);
+            atomicAdd(tm + slot, m);
+            return;
         }
-        pending &= ~grp;
+        slot = (slot + 1u) & (kTable - 1u);
+    }
+    atomicAdd(counts + k, c);               // crowded table: straight to the grid
+    atomicAdd(mass + k, m);
+}
+
+// Sums one warp's 32 (cell, scaled mass) pairs by runs of equal cells in
+// lane order: a run's last lane holds the run's count (its length) and mass
+// (a segmented inclusive scan, five shuffles) and adds them to the table.
+// The reorder leaves a warp's cells in a few runs; a cell that appears in
+// several runs is simply added several times.  Invalid lanes carry kEmpty
+// and add nothing.
+__device__ __forceinline__ void warp_runs_add(uint32_t key, uint32_t q, unsigned lane, uint32_t* tk, uint32_t* tc,
+                                              uint32_t* tm, uint32_t* __restrict__ counts,
+                                              uint32_t* __restrict__ mass) {
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const uint32_t next = __shfl_down_sync(0xffffffffu, key, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0u || prev != key);
+    const unsigned start = 31u - __clz(heads & (0xffffffffu >> (31u - lane)));
+    uint32_t v = q;
+#pragma unroll
+    for (unsigned d = 1; d < 32u; d <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= start + d) v += x;
+    }
+    if ((lane == 31u || next != key) && key != kEmpty) table_add(tk, tc, tm, key, lane - start + 1u, v, counts, mass);
+}
+
+// Each CTA bins one contiguous chunk of slots, two slots per thread per
+// pass with every field loaded up front.  All sums are u32, so the grid
+// does not depend on the order of the additions.
+__global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, uint32_t chunk,
+                                                   uint32_t* __restrict__ counts, uint32_t* __restrict__ mass) {
+    __shared__ float s_h[FPG_MAX_LEVELS];
+    __shared__ uint32_t t_key[kTable], t_cnt[kTable], t_mass[kTable];
+    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_h[i] = lt.h[i];
+    for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
+        t_key[i] = kEmpty;
+        t_cnt[i] = 0u;
+        t_mass[i] = 0u;
+    }
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+    const uint64_t end = min(begin + chunk, (uint64_t)a.n);
+    for (uint64_t base = begin; base < end; base += 2u * blockDim.x) {  // uniform across the CTA
+        uint32_t key[2], q[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const uint64_t p = base + (uint64_t)j * blockDim.x + threadIdx.x;
+            key[j] = kEmpty;
+            q[j] = 0u;
+            if (p < end) {
+                const uint32_t f = a.flags[p];
+                const int32_t cx = a.cell_x[p], cy = a.cell_y[p];
+                const float z = a.pos_z[p], m = a.mass[p];
+                if (f & 1u) {
+                    const uint32_t ix = (uint32_t)min(max(cx, 0), (int)a.nx - 1);
+                    const uint32_t iy = (uint32_t)min(max(cy, 0), (int)a.ny - 1);
+                    key[j] = (ix * a.ny + iy) * a.nz + level_of(z, s_h, a.nz, a.meters);
+                    q[j] = quantize(fmaxf(m, 0.0f), a.mass_scale);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) warp_runs_add(key[j], q[j], lane, t_key, t_cnt, t_mass, counts, mass);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
+        const uint32_t k = t_key[i];
+        if (k != kEmpty) {
+            atomicAdd(counts + k, t_cnt[i]);
+            atomicAdd(mass + k, t_mass[i]);
+        }
     }
 }
 
@@ -111,20 +178,41 @@ extern "C" fpg_status fpg_grid_create(fpg_ctx* ctx, size_t nx, size_t ny, size_t
     if (e == cudaSuccess) e = cudaMalloc(&g->mass, cells * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemsetAsync(g->counts, 0, cells * sizeof(uint32_t), ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(g->mass, 0, cells * sizeof(uint32_t), ctx->stream);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->produced, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->copied, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
-        cudaFree(g->counts); cudaFree(g->mass); delete g;
+        fpg_grid_destroy(g);
         return cuda_status(e);
     }
+    g->last_stream = ctx->stream;
     *out = g;
     return FPG_OK;
 }
 
 extern "C" fpg_status fpg_grid_destroy(fpg_grid* g) {
     if (!g) return FPG_OK;
+    if (g->copy_pending) cudaEventSynchronize(g->copied);
     cudaFree(g->counts);
     cudaFree(g->mass);
+    if (g->produced) cudaEventDestroy(g->produced);
+    if (g->copied) cudaEventDestroy(g->copied);
     delete g;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_grid_download_async(fpg_grid* g, uint32_t* counts, uint32_t* mass_scaled, void* stream) {
+    if (!g) return FPG_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = g->ctx->pick(stream);
+    const size_t cells = g->nx * g->ny * g->nz;
+    if (s != g->last_stream) {
+        FPG_CUDA(cudaEventRecord(g->produced, g->last_stream));
+        FPG_CUDA(cudaStreamWaitEvent(s, g->produced, 0));
+    }
+    if (counts) FPG_CUDA(cudaMemcpyAsync(counts, g->counts, cells * 4, cudaMemcpyDeviceToHost, s));
+    if (mass_scaled) FPG_CUDA(cudaMemcpyAsync(mass_scaled, g->mass, cells * 4, cudaMemcpyDeviceToHost, s));
+    FPG_CUDA(cudaEventRecord(g->copied, s));
+    g->copy_pending = true;
     return FPG_OK;
 }
 
@@ -137,11 +225,21 @@ extern "C" fpg_status fpg_grid_accumulate(fpg_ctx* ctx, const fpg_particles* P, 
     if (st != FPG_OK) return st;
     cudaStream_t s = ctx->pick(stream);
     const size_t cells = g->nx * g->ny * g->nz;
+    if (g->copy_pending) {                  // an fpg_grid_download_async still reading the grid
+        FPG_CUDA(cudaStreamWaitEvent(s, g->copied, 0));
+        g->copy_pending = false;
+    }
+    g->last_stream = s;
     FPG_CUDA(cudaMemsetAsync(g->counts, 0, cells * sizeof(uint32_t), s));   // outputs.clear (gridding.rs:282)
     FPG_CUDA(cudaMemsetAsync(g->mass, 0, cells * sizeof(uint32_t), s));
     g->mass_scale = mass_scale;
     if (a.n == 0) return FPG_OK;
-    grid_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(a, lt, g->counts, g->mass);
+    // 8 resident CTAs per SM, one contiguous chunk each
+    const uint32_t tiles = (uint32_t)(((uint64_t)a.n + 511u) / 512u);
+    const uint32_t ctas = std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count * 8u);
+    const uint32_t chunk = ((tiles + ctas - 1u) / ctas) * 512u;
+    const uint32_t blocks = (uint32_t)(((uint64_t)a.n + chunk - 1u) / chunk);
+    grid_kernel<<<blocks, 256, 0, s>>>(a, lt, chunk, g->counts, g->mass);
     ctx->count();
     FPG_CHECK_LAUNCH();
     return FPG_OK;

@@ -107,6 +107,7 @@ _sig("fpg_compact", _i32, _vp, _vp, _vp, _u32p, _vp, _vp)
 _sig("fpg_philox_uniforms", _i32, _vp, _u32p, _u32p, _sz, _vp, _vp, _vp)
 _sig("fpg_compaction_indices_static", _i32, _vp, _vp, _sz, _vp, _vp, _vp)
 _sig("fpg_dispatch_hanna_params", _i32, _vp, _vp, _vp, _vp, _sz, _vp)
+_sig("fpg_grid_download_async", _i32, _vp, _vp, _vp, _vp)
 _sig("fpg_cbl_sample", _i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp)
 _sig("fpg_cbl_sample_philox", _i32, _vp, _vp, _vp, _u32p, _u32p, _vp, _vp)
 _sig("fpg_convection_build_chain", _i32, _vp, _f32, _vp, _vp, _vp, _vp, _vp)
@@ -188,7 +189,7 @@ EXPORTED = [
     "fpg_step_params_default", "fpg_step", "fpg_advect_dual_wind", "fpg_langevin_fused",
     "fpg_dry_deposition", "fpg_wet_deposition",
     "fpg_grid_create", "fpg_grid_destroy", "fpg_grid_accumulate", "fpg_grid_cell_indices", "fpg_grid_download",
-    "fpg_grid_counts_device", "fpg_grid_mass_device",
+    "fpg_grid_counts_device", "fpg_grid_mass_device", "fpg_grid_download_async",
     "fpg_compaction_create", "fpg_compaction_destroy", "fpg_compact",
     "fpg_philox_uniforms",
     "fpg_compaction_indices_static",

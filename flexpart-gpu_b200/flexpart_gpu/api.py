@@ -340,6 +340,13 @@ class Grid:
                                         0 if oh is None else oh.size, _vp(out.ptr), None), "fpg_grid_cell_indices")
         return out.numpy()[:n]
 
+    def download_async(self, counts_ptr: int | None, mass_ptr: int | None, stream=None):
+        """Enqueue the copy of counts and scaled masses into host memory at the
+        given addresses (page-locked for overlap) on `stream`, ordered after
+        the last accumulate; returns at once (fpg_grid_download_async)."""
+        check(lib.fpg_grid_download_async(self.h, _vp(counts_ptr) if counts_ptr else None,
+                                          _vp(mass_ptr) if mass_ptr else None, stream), "fpg_grid_download_async")
+
     def download(self):
         n = self.shape[0] * self.shape[1] * self.shape[2]
         counts = np.empty(n, np.uint32)

@@ -381,6 +381,13 @@ fpg_status fpg_grid_accumulate(fpg_ctx* ctx, const fpg_particles* particles, fpg
 fpg_status fpg_grid_cell_indices(fpg_ctx* ctx, const fpg_particles* particles, const fpg_grid* grid,
                                  const float* outheights, size_t n_outheights, uint32_t* out_dev,
                                  void* stream);
+/* The counts and raw scaled masses copied to host memory (page-locked for
+ * overlap, e.g. fpg_host_alloc) on `stream` without waiting: the copy is
+ * ordered after the grid's last accumulate, and the next accumulate into
+ * this grid waits for it.  The host buffers are complete once `stream`
+ * reaches this point (synchronize it, or make another stream wait on it).
+ * Either pointer may be NULL. */
+fpg_status fpg_grid_download_async(fpg_grid* grid, uint32_t* counts, uint32_t* mass_scaled, void* stream);
 /* download_output (gridding.rs:191-219): counts, raw scaled masses and kg
  * (= scaled / mass_scale as f32); any pointer may be NULL. */
 fpg_status fpg_grid_download(fpg_grid* g, uint32_t* counts, uint32_t* mass_scaled, float* mass_kg,

@@ -239,7 +239,7 @@ def test_convective_mixing_matches_the_reference_chain_test(ctx):
 def test_convective_mixing_bit_exact_on_a_million_slots(ctx):
     from flexpart_gpu import convection as cv
     rng = np.random.default_rng(4)
-    n = 1_000_000
+    n = 1_000_003                                                      # a ragged last quad
     z = rng.uniform(-1000.0, 6000.0, n).astype(np.float32)
     z[:8] = np.float32(IFACE + [np.nan, np.inf])[:8]
     rec = _records(np.c_[np.full(n, 0.5), np.full(n, 0.5), z], (rng.random(n) > 0.25).astype(np.uint32))

@@ -110,3 +110,34 @@ def test_sort_by_cell_matches_oracle_permutation(ctx, n, heights):
     srt.sort(p, m)
     ref2, _ = orc.sort_by_cell(rec, n // 2, met["heights"], (spec.nx, spec.ny, spec.nz))
     assert np.array_equal(p.download(), ref2)
+
+
+def test_async_grid_download_orders_against_the_next_accumulate(ctx):
+    """fpg_grid_download_async on a side stream into page-locked memory: the
+    copy sees the grid of the accumulate before it, and the next accumulate
+    into the same grid does not overwrite it before the copy is done."""
+    import ctypes
+
+    import torch
+
+    nx, ny = 40, 30
+    oh = [100.0, 500.0, 1000.0]
+    ra = population(nx, ny, 300_000, seed=5, z_max=2000.0)
+    rb = population(nx, ny, 300_000, seed=6, z_max=2000.0)
+    pa, pb = api.Particles(ctx, len(ra)), api.Particles(ctx, len(rb))
+    pa.upload(ra)
+    pb.upload(rb)
+    g = api.Grid(ctx, nx, ny, 3)
+    cells = nx * ny * 3
+    side = torch.cuda.Stream()
+    bufs = [torch.zeros(cells, dtype=torch.int32, pin_memory=True) for _ in range(4)]
+    g.accumulate(pa, 0, 1e6, oh)
+    g.download_async(bufs[0].data_ptr(), bufs[1].data_ptr(), ctypes.c_void_p(side.cuda_stream))
+    g.accumulate(pb, 0, 1e6, oh)
+    g.download_async(bufs[2].data_ptr(), bufs[3].data_ptr(), ctypes.c_void_p(side.cuda_stream))
+    side.synchronize()
+    ctx.synchronize()
+    for rec, c, m in ((ra, bufs[0], bufs[1]), (rb, bufs[2], bufs[3])):
+        oc, om, _ = orc.grid(orc.State.from_records(rec), len(rec), 0, 1e6, oh, (nx, ny, 3))
+        assert np.array_equal(c.numpy().view(np.uint32), oc)
+        assert np.array_equal(m.numpy().view(np.uint32), om)
