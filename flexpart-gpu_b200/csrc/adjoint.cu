@@ -256,16 +256,49 @@ __device__ __forceinline__ void warp_sum24(float (&v)[24], unsigned lane) {
     }
 }
 
+// The CTA's table of bias-gradient nodes for one adjoint step: open
+// addressing on the node index in shared memory, three float sums per node,
+// added to the f64 gradient once per node per CTA at the end of the step.
+// The f64 atomics of the per-warp sums were the cost of the whole reverse
+// sweep (two thirds of it); the table takes them off the L2.
+constexpr uint32_t kBiasTableBits = 10;
+constexpr uint32_t kBiasTable = 1u << kBiasTableBits;
+constexpr uint32_t kBiasProbes = 8;
+constexpr uint32_t kBiasEmpty = 0xffffffffu;
+
+struct BiasTable {
+    uint32_t* key;   // kBiasTable
+    float* g;        // 3 * kBiasTable
+};
+
+__device__ __forceinline__ void bias_add(const BiasTable& t, uint32_t n, float gu, float gv, float gw,
+                                         double* __restrict__ dbias) {
+    uint32_t slot = (n * 2654435761u) >> (32 - kBiasTableBits);
+    for (uint32_t i = 0; i < kBiasProbes; ++i) {
+        const uint32_t old = atomicCAS(t.key + slot, kBiasEmpty, n);
+        if (old == kBiasEmpty || old == n) {
+            atomicAdd(t.g + 3u * slot + 0u, gu);
+            atomicAdd(t.g + 3u * slot + 1u, gv);
+            atomicAdd(t.g + 3u * slot + 2u, gw);
+            return;
+        }
+        slot = (slot + 1u) & (kBiasTable - 1u);
+    }
+    atomicAdd(dbias + 3u * n + 0u, (double)gu);     // crowded table: straight to the gradient
+    atomicAdd(dbias + 3u * n + 1u, (double)gv);
+    atomicAdd(dbias + 3u * n + 2u, (double)gw);
+}
+
 // Vector-Jacobian product of one dual-time trilinear sample: given lambda of
 // its (u, v, w), returns lambda . d(u, v, w)/d(x, y, z) and adds lambda x
 // corner weight to the bias gradient of each corner node (the bias enters
 // both frames, whose time weights sum to one).  Called by the whole warp;
 // lanes with valid == false contribute nothing.  The bias terms of lanes
 // whose samples share a corner set are summed across the warp first, and
-// eight lanes then issue one corner's three atomics each.
+// eight lanes then add one corner each to the CTA's table.
 __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts, bool valid, float x, float y,
                                              float z, float alpha, float lu, float lv, float lw,
-                                             double* __restrict__ dbias) {
+                                             double* __restrict__ dbias, const BiasTable& table) {
     uint32_t x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
     axis_bracket(x, a.nx, x0, x1, tx);
@@ -279,6 +312,9 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts
     const uint32_t xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
     const float wx[2] = {1.0f - tx, tx}, wy[2] = {1.0f - ty, ty}, wz[2] = {1.0f - tz, tz};
     const float ta = 1.0f - alpha;
+    // a lane whose lambda is zero (a particle that reaches no receptor after
+    // this step) adds nothing: it loads no corners and joins no group
+    const bool act = valid && (lu != 0.0f || lv != 0.0f || lw != 0.0f);
     float f[2][2][2];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -287,7 +323,7 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 float fv = 0.0f;
-                if (valid) {
+                if (act) {
                     const Node v = ld_node(a.bracket, (xs[i] * a.ny + ys[j]) * a.nz + zs[k]);
                     fv = lu * (ta * v.u0 + alpha * v.u1) + lv * (ta * v.v0 + alpha * v.v1) +
                          lw * (ta * v.w0 + alpha * v.w1);
@@ -295,13 +331,13 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts
                 f[i][j][k] = fv;
             }
     if (dbias) {
-        const uint32_t key = valid ? (x0 * a.ny + y0) * a.nz + z0 : 0xffffffffu;
+        const uint32_t key = act ? (x0 * a.ny + y0) * a.nz + z0 : 0xffffffffu;
         const unsigned lane = threadIdx.x & 31u;
-        unsigned pending = __ballot_sync(0xffffffffu, valid);
+        unsigned pending = __ballot_sync(0xffffffffu, act);
         while (pending) {
             const int src = __ffs(pending) - 1;
             const uint32_t k0 = __shfl_sync(0xffffffffu, key, src);
-            const bool mine = valid && key == k0;
+            const bool mine = act && key == k0;
             const unsigned grp = __ballot_sync(0xffffffffu, mine);
             float v[24];
 #pragma unroll
@@ -318,9 +354,7 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts
                 const uint32_t bx = k0 / (a.ny * a.nz), by = (k0 / a.nz) % a.ny, bz = k0 % a.nz;
                 const uint32_t n = (((c >> 2) ? cx : bx) * a.ny + (((c >> 1) & 1u) ? cy : by)) * a.nz +
                                    ((c & 1u) ? cz : bz);
-                atomicAdd(dbias + 3u * n + 0u, (double)v[0]);
-                atomicAdd(dbias + 3u * n + 1u, (double)v[1]);
-                atomicAdd(dbias + 3u * n + 2u, (double)v[2]);
+                bias_add(table, n, v[0], v[1], v[2], dbias);
             }
             pending &= ~grp;
         }
@@ -373,7 +407,16 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
                                                                  double* __restrict__ dsrc) {
     extern __shared__ float s_heights[];
     __shared__ uint32_t s_item;
+    __shared__ uint32_t s_bias_key[kBiasTable];
+    __shared__ float s_bias_g[3 * kBiasTable];
     for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
+    for (uint32_t i = threadIdx.x; i < kBiasTable; i += blockDim.x) {
+        s_bias_key[i] = kBiasEmpty;
+        s_bias_g[3u * i] = 0.0f;
+        s_bias_g[3u * i + 1u] = 0.0f;
+        s_bias_g[3u * i + 2u] = 0.0f;
+    }
+    const BiasTable table{s_bias_key, s_bias_g};
     const float alpha = st->alpha;
     const bool output = r.every != 0 && (st->step + 1u) % r.every == 0u;
     const float kx = a.xs * a.dt, ky = a.ys * a.dt, kz = a.zs * a.dt;
@@ -427,7 +470,7 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
         const float lu1 = lu0, lv1 = lv0, lw1 = lw0;
         ltu0 += lu1;
         ltv0 += lv1;
-        const float3 g1 = sample_vjp(a, s_heights, valid, px, py, pz, alpha, lu1, lv1, lw1, dbias);
+        const float3 g1 = sample_vjp(a, s_heights, valid, px, py, pz, alpha, lu1, lv1, lw1, dbias, table);
         const float gpx = (fl & ADV_PX) ? g1.x : 0.0f;
         const float gpy = (fl & ADV_PY) ? g1.y : 0.0f;
         const float gpz = (fl & ADV_PZ) ? g1.z : 0.0f;
@@ -436,7 +479,7 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
         lz0 += gpz; lw0 += gpz * kz;
         ltu0 += lu0;
         ltv0 += lv0;
-        const float3 g0 = sample_vjp(a, s_heights, valid, x0, y0, z0, alpha, lu0, lv0, lw0, dbias);
+        const float3 g0 = sample_vjp(a, s_heights, valid, x0, y0, z0, alpha, lu0, lv0, lw0, dbias, table);
         lx0 += g0.x; ly0 += g0.y; lz0 += g0.z;
         if (valid) {
             lam.f[L_X][p] = lx0; lam.f[L_Y][p] = ly0; lam.f[L_Z][p] = lz0;
@@ -454,6 +497,18 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
                 atomicAdd(g + 1, (double)sy);
                 atomicAdd(g + 2, (double)sz);
                 atomicAdd(g + 3, (double)sm);
+            }
+        }
+    }
+    // the loop ends for the whole CTA together: flush the bias table
+    if (dbias) {
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kBiasTable; i += blockDim.x) {
+            const uint32_t n = s_bias_key[i];
+            if (n != kBiasEmpty) {
+                atomicAdd(dbias + 3u * n + 0u, (double)s_bias_g[3u * i]);
+                atomicAdd(dbias + 3u * n + 1u, (double)s_bias_g[3u * i + 1u]);
+                atomicAdd(dbias + 3u * n + 2u, (double)s_bias_g[3u * i + 2u]);
             }
         }
     }
@@ -508,6 +563,9 @@ struct InverseData {
     uint2* items = nullptr;              // 256-slot work items
     uint32_t n_items = 0;
     uint32_t* work = nullptr;
+    uint32_t* work_rev = nullptr;        // one work counter per tape slice for the reverse sweep
+    // start time of the met bracket packed in device memory (INT64_MIN: unknown)
+    int64_t packed_ta = INT64_MIN;
     bool forward_done = false;
     uint64_t bytes = 0;
     uint32_t grid_tape = 0, grid_adj = 0;  // persistent grids: SMs x resident CTAs
@@ -594,6 +652,7 @@ static fpg_status rebuild_ring(fpg_inverse* v) {
     v->b->ctx->count(1);
     FPG_CHECK_LAUNCH();
     v->d.forward_done = false;
+    v->d.packed_ta = INT64_MIN;             // the ring changed under the packed bracket
     return FPG_OK;
 }
 
@@ -645,7 +704,7 @@ extern "C" fpg_status fpg_inverse_destroy(fpg_inverse* v) {
     cudaFree(d.rmap); cudaFree(d.sim); cudaFree(d.g); cudaFree(d.ring_raw); cudaFree(d.bias);
     cudaFree(d.ckpt); cudaFree(d.ckpt_st); cudaFree(d.ckpt_sc); cudaFree(d.st_all); cudaFree(d.sc_all);
     cudaFree(d.tape); cudaFree(d.lam); cudaFree(d.dbias); cudaFree(d.dbias_f); cudaFree(d.dsrc);
-    cudaFree(d.items); cudaFree(d.work);
+    cudaFree(d.items); cudaFree(d.work); cudaFree(d.work_rev);
     fpg_batch_destroy(v->b);
     delete v;
     return FPG_OK;
@@ -710,6 +769,7 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = alloc((void**)&d.dsrc, n_src * 4 * 8);
     if (e == cudaSuccess) e = alloc((void**)&d.items, items.size() * sizeof(uint2));
     if (e == cudaSuccess) e = alloc((void**)&d.work, 4);
+    if (e == cudaSuccess) e = alloc((void**)&d.work_rev, (size_t)K * 4);
     cudaStream_t s = ctx->stream;
     if (e == cudaSuccess) e = cudaMemcpyAsync(d.rmap, rmap.data(), rmap.size() * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
@@ -774,6 +834,16 @@ extern "C" fpg_status fpg_inverse_set_sources(fpg_inverse* v, const double* mass
     return FPG_OK;
 }
 
+// Start of the met bracket that step k runs in: batch_advance_kernel's
+// formula at t = start + k dt (at a frame time the bracket ending there).
+static int64_t step_bracket_start(const fpg_batch* b, uint64_t k) {
+    const int64_t start = b->cfg.start_seconds, fs = b->cfg.frame_seconds;
+    const int64_t t = start + (int64_t)k * b->cfg.timestep_seconds;
+    int64_t i = (t - start) / fs;
+    if (t - start == i * fs && i > 0) i -= 1;
+    return start + i * fs;
+}
+
 extern "C" fpg_status fpg_inverse_forward(fpg_inverse* v, double* simulated) {
     if (!v) return FPG_ERR_INVALID_ARGUMENT;
     fpg_batch* b = v->b;
@@ -798,6 +868,8 @@ extern "C" fpg_status fpg_inverse_forward(fpg_inverse* v, double* simulated) {
         }
     }
     b->steps_done = b->total_steps;
+    // the step kernels left the bracket of the last step packed
+    if (b->total_steps) d.packed_ta = step_bracket_start(b, b->total_steps - 1);
     if (simulated && !d.receptors.empty())
         FPG_CUDA(cudaMemcpyAsync(simulated, d.sim, d.receptors.size() * 8, cudaMemcpyDeviceToHost, s));
     FPG_CUDA(cudaStreamSynchronize(s));
@@ -835,21 +907,28 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
     for (int64_t w = windows - 1; w >= 0; --w) {
         const uint64_t k0 = (uint64_t)w * K, k1 = std::min<uint64_t>(k0 + K, n);
         if (!d.tape_in_forward) {
-            // taped recompute of the window from its checkpoint
+            // taped recompute of the window from its checkpoint; it leaves the
+            // bracket of its last step packed
             FPG_CUDA(restore_checkpoint(v, (uint32_t)w));
             for (uint64_t k = k0; k < k1; ++k) {
                 FPG_CUDA(cudaGraphLaunch(d.tape_exec[0], s));
                 b->ctx->count(d.tape_launches[0]);
             }
+            d.packed_ta = step_bracket_start(b, k1 - 1);
         }
-        // reverse of the window
+        // one work counter per slice of the window, cleared once
+        FPG_CUDA(cudaMemsetAsync(d.work_rev, 0, (size_t)K * 4, s));
+        // reverse of the window; the bracket is repacked only where it changes
         for (uint64_t k = k1; k-- > k0;) {
             const uint32_t j = (uint32_t)(k % K);
-            enqueue_pack_forced(b, d.st_all + j, s);
-            FPG_CUDA(cudaMemsetAsync(d.work, 0, 4, s));
+            const int64_t ta = step_bracket_start(b, k);
+            if (ta != d.packed_ta) {
+                enqueue_pack_forced(b, d.st_all + j, s);
+                d.packed_ta = ta;
+            }
             inverse_adjoint_kernel<<<d.grid_adj, 256, smem, s>>>(a, d.st_all + j, d.sc_all + (size_t)j * n_src,
-                                                                 d.items, d.n_items, d.work, tb, j, lam, rargs,
-                                                                 d_bias ? d.dbias : nullptr, d.dsrc);
+                                                                 d.items, d.n_items, d.work_rev + j, tb, j, lam,
+                                                                 rargs, d_bias ? d.dbias : nullptr, d.dsrc);
             b->ctx->count(1);
             FPG_CHECK_LAUNCH();
         }
