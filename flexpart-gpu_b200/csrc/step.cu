@@ -530,6 +530,98 @@ extern "C" fpg_status fpg_langevin_fused(fpg_ctx* ctx, fpg_particles* particles,
     return fpg_step(ctx, particles, nullptr, pbl, &p, next_counter, stream);
 }
 
+namespace fpg {
+namespace {
+
+struct RecordTurbArgs {
+    float* pos_z;
+    float* turb_u;
+    float* turb_v;
+    float* turb_w;
+    int32_t* cbt;
+    const uint32_t* flags;
+    const fpg_hanna_params* hanna;
+    uint32_t n;
+    float tdt, rho, zmin;
+    uint32_t n_sub;
+    u32x4 counter;
+    uint32_t key0, key1;
+};
+
+// langevin.wgsl:307-424: the turbulence update from a HannaParams record per
+// slot (the separated Hanna -> Langevin path of the reference's validation
+// and backward loops), with the fused kernel's Philox block layout and
+// Gaussian assignment.
+__global__ void __launch_bounds__(256) langevin_record_kernel(RecordTurbArgs a) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n || !(a.flags[p] & FLAG_ACTIVE)) return;
+    const uint32_t n_vert = a.n_sub > 1u ? a.n_sub : 1u;
+    const uint32_t blocks = (2u + n_vert + 3u) / 4u;
+    const u32x4 b0 = philox4x32_10(counter_add(a.counter, p * blocks), a.key0, a.key1);
+    u32x4 b1 = {0u, 0u, 0u, 0u};
+    if (blocks > 1u) b1 = philox4x32_10(counter_add(a.counter, p * blocks + 1u), a.key0, a.key1);
+    const float2 e_uv = box_muller(u32_to_uniform01(b0.x), u32_to_uniform01(b0.y));
+    const float2 e_w01 = box_muller(u32_to_uniform01(b0.z), u32_to_uniform01(b0.w));
+    const float2 e_w23 = box_muller(u32_to_uniform01(b1.x), u32_to_uniform01(b1.y));
+    const fpg_hanna_params& r = a.hanna[p];
+    Hanna hn;
+    hn.ust = r.ust; hn.wst = r.wst; hn.ol = r.ol; hn.h = r.h;
+    hn.sigu = r.sigu; hn.sigv = r.sigv; hn.sigw = r.sigw; hn.dsigwdz = r.dsigwdz;
+    hn.tlu = r.tlu; hn.tlv = r.tlv; hn.tlw = r.tlw;
+    // the branch hanna_short_w takes: its test on (L, max(h, 1))
+    hn.regime = hanna_regime(r.ol, fmaxf(r.h, 1.0f));
+    float pz = a.pos_z[p], tu = a.turb_u[p], tv = a.turb_v[p], tw = a.turb_w[p];
+    const int32_t cbt_in = a.n_sub == 0u ? 0 : a.cbt[p];
+    int32_t cbt = cbt_in;
+    turbulence_from_hanna<float, RecordLangevin>(a, hn, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
+    a.turb_u[p] = tu; a.turb_v[p] = tv; a.turb_w[p] = tw;
+    if (a.n_sub != 0u) {
+        a.pos_z[p] = pz;
+        if (cbt != cbt_in) a.cbt[p] = cbt;
+    }
+}
+
+}  // namespace
+}  // namespace fpg
+
+extern "C" fpg_status fpg_langevin_with_hanna(fpg_ctx* ctx, fpg_particles* P, const fpg_hanna_params* hanna_dev,
+                                              size_t n_hanna, float dt, float rho_grad_over_rho, uint32_t n_substeps,
+                                              float min_height_m, const uint32_t key[2],
+                                              const uint32_t base_counter[4], uint32_t next_counter[4],
+                                              void* stream) {
+    if (!ctx || !P || !key || !base_counter) return FPG_ERR_INVALID_ARGUMENT;
+    const size_t n = P->dispatch;
+    if (next_counter) std::memcpy(next_counter, base_counter, sizeof(uint32_t) * 4);
+    // encode_update_particles_turbulence_langevin_gpu_with_hanna_buffer_and_kernel
+    // (src/gpu/langevin.rs:248-329): MismatchedInputLengths, empty, InvalidTimeStep
+    if (n_hanna != n) return FPG_ERR_LENGTH_MISMATCH;
+    if (n == 0) return FPG_OK;
+    if (!std::isfinite(dt) || dt <= 0.0f) return FPG_ERR_INVALID_TIME_STEP;
+    if (n > (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    if (!hanna_dev) return FPG_ERR_INVALID_ARGUMENT;
+    RecordTurbArgs a{};
+    a.pos_z = static_cast<float*>(P->field[FPG_FIELD_POS_Z]);
+    a.turb_u = static_cast<float*>(P->field[FPG_FIELD_TURB_U]);
+    a.turb_v = static_cast<float*>(P->field[FPG_FIELD_TURB_V]);
+    a.turb_w = static_cast<float*>(P->field[FPG_FIELD_TURB_W]);
+    a.cbt = static_cast<int32_t*>(P->field[FPG_FIELD_CBT]);
+    a.flags = static_cast<const uint32_t*>(P->field[FPG_FIELD_FLAGS]);
+    a.hanna = hanna_dev;
+    a.n = (uint32_t)n;
+    a.tdt = dt;
+    a.rho = rho_grad_over_rho;
+    a.zmin = min_height_m;
+    a.n_sub = n_substeps;
+    a.counter = u32x4{base_counter[0], base_counter[1], base_counter[2], base_counter[3]};
+    a.key0 = key[0];
+    a.key1 = key[1];
+    langevin_record_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->pick(stream)>>>(a);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
+    if (next_counter) counter_add64(base_counter, (uint64_t)n * (n_substeps <= 2u ? 1u : 2u), next_counter);
+    return FPG_OK;
+}
+
 extern "C" fpg_status fpg_dry_deposition(fpg_ctx* ctx, fpg_particles* particles, const float* vdep_dev, float dt,
                                          float href, float* prob_dev, void* stream) {
     if (!vdep_dev) return FPG_ERR_INVALID_ARGUMENT;

@@ -144,19 +144,48 @@ __device__ __forceinline__ void split_coord(float coord, uint32_t n, int32_t& ce
     frac = f;
 }
 
-// Turbulence of one particle (langevin_fused.wgsl:414-515 after the PBL
-// lookup and the noise draws): Hanna at the particle height, horizontal
-// Langevin updates, then the vertical sub-steps with ground and PBL-top
-// reflection.  A template over the scalar type: float for the step, the
-// dual number of the adjoint for its Jacobian (same values, bit for bit).
-template <class T>
-__device__ __forceinline__ void turbulence_update(const StepArgs& a, float4 cell, float2 e_uv, float2 e_w01,
-                                                  float2 e_w23, T& pz, T& tu, T& tv, T& tw, int32_t& cbt) {
-    const HannaT<T> hn = compute_hanna_t<T>(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
-    tu = langevin_h_t<T>(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
-    tv = langevin_h_t<T>(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
+// The Langevin updates as the fused shader applies them to Hanna outputs
+// (sigma >= 0.01 and T_L >= 10 s by construction).
+struct HannaLangevin {
+    template <class T>
+    __device__ static __forceinline__ T h(T prev, T sigma, T tl, float dt, float eta) {
+        return langevin_h_t<T>(prev, sigma, tl, dt, eta);
+    }
+    template <class T>
+    __device__ static __forceinline__ T v(T prev, T sigma_w, T tlw, T dsigwdz, float dt, float rho, float eta) {
+        return langevin_v_t<T>(prev, sigma_w, tlw, dsigwdz, dt, rho, eta);
+    }
+};
+
+// The same updates on caller-supplied HannaParams records (langevin.wgsl:
+// 189-238, physics/langevin.rs:116-121,146-150): sigma and T_L pass through
+// sanitize_positive and a zero T_L gives zero turbulence.  Float only.
+struct RecordLangevin {
+    __device__ static __forceinline__ float h(float prev, float sigma, float tl, float dt, float eta) {
+        const float s = sanitize_positive(sigma), t = sanitize_positive(tl);
+        return t == 0.0f ? 0.0f : langevin_h_t<float>(prev, s, t, dt, eta);
+    }
+    __device__ static __forceinline__ float v(float prev, float sigma_w, float tlw, float dsigwdz, float dt,
+                                              float rho, float eta) {
+        const float s = sanitize_positive(sigma_w), t = sanitize_positive(tlw);
+        return t == 0.0f ? 0.0f : langevin_v_t<float>(prev, s, t, dsigwdz, dt, rho, eta);
+    }
+};
+
+// Turbulence of one particle from its Hanna parameters
+// (langevin_fused.wgsl:446-515, langevin.wgsl:350-421): horizontal Langevin
+// updates, then the vertical sub-steps with ground and PBL-top reflection and
+// the vertical Hanna re-evaluation between sub-steps.  A template over the
+// scalar type (float for the step, the dual number of the adjoint for its
+// Jacobian: same values, bit for bit), the update policy and the argument
+// block (any type with tdt, rho, zmin and n_sub).
+template <class T, class L, class A>
+__device__ __forceinline__ void turbulence_from_hanna(const A& a, const HannaT<T>& hn, float2 e_uv, float2 e_w01,
+                                                      float2 e_w23, T& pz, T& tu, T& tv, T& tw, int32_t& cbt) {
+    tu = L::h(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
+    tv = L::h(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
     if (a.n_sub == 0u) {
-        tw = langevin_v_t<T>(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
+        tw = L::v(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
         return;
     }
     const float dt_sub = a.tdt / (float)a.n_sub;
@@ -165,7 +194,7 @@ __device__ __forceinline__ void turbulence_update(const StepArgs& a, float4 cell
     T sigw = hn.sigw, dsigwdz = hn.dsigwdz, tlw = hn.tlw;
     for (uint32_t sub = 0; sub < a.n_sub; ++sub) {
         const float eta = sub == 0u ? e_w01.x : sub == 1u ? e_w01.y : sub == 2u ? e_w23.x : e_w23.y;
-        tw = langevin_v_t<T>(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
+        tw = L::v(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
         pz = pz + tw * dt_sub;
         if (h > zmin) {
             T z = pz;
@@ -178,6 +207,16 @@ __device__ __forceinline__ void turbulence_update(const StepArgs& a, float4 cell
         }
         if (sub < a.n_sub - 1u) hanna_short_w_t<T>(hn.ust, hn.wst, hn.ol, hn.h, pz, hn.regime, sigw, dsigwdz, tlw);
     }
+}
+
+// Turbulence of one particle in the fused step (langevin_fused.wgsl:414-515
+// after the PBL lookup and the noise draws): Hanna at the particle height,
+// then turbulence_from_hanna.
+template <class T>
+__device__ __forceinline__ void turbulence_update(const StepArgs& a, float4 cell, float2 e_uv, float2 e_w01,
+                                                  float2 e_w23, T& pz, T& tu, T& tv, T& tw, int32_t& cbt) {
+    const HannaT<T> hn = compute_hanna_t<T>(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
+    turbulence_from_hanna<T, HannaLangevin>(a, hn, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
 }
 
 // What the step records for its adjoint (a policy of particle_step): NoTape

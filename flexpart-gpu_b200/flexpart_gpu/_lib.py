@@ -108,6 +108,7 @@ _sig("fpg_philox_uniforms", _i32, _vp, _u32p, _u32p, _sz, _vp, _vp, _vp)
 _sig("fpg_compaction_indices_static", _i32, _vp, _vp, _sz, _vp, _vp, _vp)
 _sig("fpg_dispatch_hanna_params", _i32, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("fpg_grid_download_async", _i32, _vp, _vp, _vp, _vp)
+_sig("fpg_langevin_with_hanna", _i32, _vp, _vp, _vp, _sz, _f32, _f32, _u32, _f32, _u32p, _u32p, _u32p, _vp)
 _sig("fpg_cbl_sample", _i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp)
 _sig("fpg_cbl_sample_philox", _i32, _vp, _vp, _vp, _u32p, _u32p, _vp, _vp)
 _sig("fpg_convection_build_chain", _i32, _vp, _f32, _vp, _vp, _vp, _vp, _vp)
@@ -194,7 +195,7 @@ EXPORTED = [
     "fpg_philox_uniforms",
     "fpg_compaction_indices_static",
     "fpg_sorter_create", "fpg_sorter_destroy", "fpg_sort_by_cell",
-    "fpg_dispatch_hanna_params", "fpg_cbl_sample", "fpg_cbl_sample_philox",
+    "fpg_dispatch_hanna_params", "fpg_langevin_with_hanna", "fpg_cbl_sample", "fpg_cbl_sample_philox",
     "fpg_convection_build_chain", "fpg_convection_level_index", "fpg_convection_apply_profile",
     "fpg_convection_create", "fpg_convection_destroy", "fpg_convection_set_matrix", "fpg_convection_heights",
     "fpg_convective_mixing",

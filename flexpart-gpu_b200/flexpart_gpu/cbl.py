@@ -6,6 +6,9 @@ Mirrors the reference's GPU entry points:
 * ``dispatch_hanna_params_gpu`` / ``compute_hanna_params_gpu``
   (src/gpu/hanna.rs:212-330): one HannaParams record per slot from the PBL
   fields at the particle's cell;
+* ``update_particles_turbulence_langevin_gpu`` (src/gpu/langevin.rs:
+  248-329): the Langevin update from those records (the reference's
+  validation and backward path; the fused step computes the same);
 * ``sample_cbl_vertical_velocity_gpu`` (src/gpu/cbl.rs:189-319): the
   bi-Gaussian PDF of w' and one sample per slot from caller uniforms;
 * ``sample_cbl_vertical_velocity_philox``: the same sample with sigma_w
@@ -20,6 +23,8 @@ ZeroPblShape -> ZERO_SHAPE).
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from ._lib import check, lib
@@ -28,7 +33,8 @@ from .records import CBL_INPUT_DTYPE, CBL_OUTPUT_DTYPE, HANNA_PARAMS_DTYPE
 
 __all__ = [
     "HANNA_PARAMS_DTYPE", "CBL_INPUT_DTYPE", "CBL_OUTPUT_DTYPE", "sampling_inputs",
-    "dispatch_hanna_params_gpu", "compute_hanna_params_gpu", "sample_cbl_vertical_velocity_gpu",
+    "dispatch_hanna_params_gpu", "compute_hanna_params_gpu", "update_particles_turbulence_langevin_gpu",
+    "sample_cbl_vertical_velocity_gpu",
     "sample_cbl_vertical_velocity_philox",
 ]
 
@@ -60,6 +66,21 @@ def compute_hanna_params_gpu(ctx: Context, particles: Particles, pbl: Pbl) -> np
     if particles.dispatch_count == 0:
         return np.zeros(0, HANNA_PARAMS_DTYPE)
     return dispatch_hanna_params_gpu(ctx, particles, pbl).numpy()
+
+
+def update_particles_turbulence_langevin_gpu(ctx: Context, particles: Particles, hanna_params, dt: float,
+                                             rho_grad_over_rho: float, n_substeps: int, min_height_m: float, key,
+                                             counter, stream=None):
+    """The Langevin update from per-slot HannaParams records (a host record
+    array or a DeviceArray of HANNA_PARAMS_DTYPE): the reference's separated
+    Hanna -> Langevin path (src/gpu/langevin.rs:248-329).  Returns the next
+    Philox counter."""
+    h_dev, n_h = _device(ctx, hanna_params, HANNA_PARAMS_DTYPE)
+    nxt = (ctypes.c_uint32 * 4)()
+    check(lib.fpg_langevin_with_hanna(ctx.h, particles.h, _vp(h_dev.ptr), n_h, dt, rho_grad_over_rho, n_substeps,
+                                      min_height_m, _u32arr(key, 2), _u32arr(counter, 4), nxt, stream),
+          "fpg_langevin_with_hanna")
+    return list(nxt)
 
 
 def _device(ctx, a, dtype):

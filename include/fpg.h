@@ -498,6 +498,21 @@ typedef struct fpg_cbl_sampling_output {
 fpg_status fpg_dispatch_hanna_params(fpg_ctx* ctx, const fpg_particles* particles, const fpg_pbl* pbl,
                                      fpg_hanna_params* out_dev, size_t n_out, void* stream);
 
+/* encode_update_particles_turbulence_langevin_gpu_with_hanna_buffer_and_kernel
+ * (src/gpu/langevin.rs:248-329, langevin.wgsl:307-424): the turbulence update
+ * of every active slot [0, dispatch_count) from its HannaParams record — the
+ * separated Hanna -> Langevin path of the reference's validation and backward
+ * loops — with the Philox block layout of fpg_langevin_fused; records from
+ * fpg_dispatch_hanna_params give the fused kernel's results bit for bit.
+ * Sigma and T_L pass through sanitize_positive and a zero T_L gives zero
+ * turbulence (langevin.wgsl:189-238).  next_counter = base + n * blocks per
+ * slot (1 for n_substeps <= 2, else 2).  Errors: MismatchedInputLengths
+ * (n_hanna != dispatch_count -> LENGTH_MISMATCH), InvalidTimeStep. */
+fpg_status fpg_langevin_with_hanna(fpg_ctx* ctx, fpg_particles* particles, const fpg_hanna_params* hanna_dev,
+                                   size_t n_hanna, float dt, float rho_grad_over_rho, uint32_t n_substeps,
+                                   float min_height_m, const uint32_t key[2], const uint32_t base_counter[4],
+                                   uint32_t next_counter[4], void* stream);
+
 /* sample_cbl_vertical_velocity_gpu (src/gpu/cbl.rs:204-319, cbl.wgsl:251-298):
  * per slot [0, dispatch_count) the CBL bi-Gaussian PDF of w' from the slot's
  * height and Hanna record (h, w*, sigma_w, L; physics/cbl.rs:126-226) and one

@@ -301,3 +301,87 @@ def test_convection_errors(ctx):
         cbl.sample_cbl_vertical_velocity_gpu(ctx, _upload(ctx, rec), np.zeros(2, cbl.HANNA_PARAMS_DTYPE),
                                              cbl.sampling_inputs([0.1] * 3, [0.2] * 3, [0.3] * 3))
     assert e.value.status == -5
+
+
+@pytest.mark.parametrize("n_substeps", [4, 2, 0])
+def test_separated_hanna_then_langevin_equals_the_fused_kernel(ctx, n_substeps):
+    """The reference's validation/backward path (hanna_params.wgsl then
+    langevin.wgsl on the record buffer) against its production path (the
+    fused kernel): with the records of fpg_dispatch_hanna_params the two
+    give the same bits, and the same next Philox counter."""
+    from flexpart_gpu import cbl
+    rng = np.random.default_rng(9)
+    nx, ny, n = 30, 20, 200_003
+    pbl, _ = _pbl(ctx, nx, ny, rng)
+    rec = _records(np.c_[rng.uniform(0, nx, n), rng.uniform(0, ny, n), rng.uniform(-5, 3000, n)],
+                   (rng.random(n) > 0.1).astype(np.uint32))
+    rec["turb_u"], rec["turb_v"], rec["turb_w"] = (rng.normal(0, 0.5, n).astype(np.float32) for _ in range(3))
+    rec["cbt"] = rng.choice([-1, 1], n).astype(np.int32)
+    key, counter = (0xDECAFBAD, 0x12345678), (0xA5A50001, 0xFACEB00C, 7, 9)
+    pa, pb = _upload(ctx, rec), _upload(ctx, rec)
+    na = api.langevin_fused(ctx, pa, pbl, 600.0, 2.5e-4, n_substeps, 0.01, key, counter)
+    hanna = cbl.dispatch_hanna_params_gpu(ctx, pb, pbl)
+    nb = cbl.update_particles_turbulence_langevin_gpu(ctx, pb, hanna, 600.0, 2.5e-4, n_substeps, 0.01, key, counter)
+    assert na == nb == orc.next_counter(list(counter), n, n_substeps)
+    assert pa.download().tobytes() == pb.download().tobytes()
+
+
+def test_langevin_with_hanna_records_matches_the_reference_legacy_case(ctx):
+    # src/gpu/langevin.rs:662-805: five particles over a 4x1 PBL (unstable,
+    # neutral, stable, unstable), the last inactive; Hanna records on the
+    # device, then the legacy Langevin step (dt 45 s, rho'/rho 2.5e-4, no
+    # sub-steps) against the oracle's turbulence at 5e-5
+    from flexpart_gpu import cbl
+    from flexpart_gpu.records import StepParams
+    rec = _records([(0.2, 0.0, 120.0), (1.1, 0.0, 80.0), (2.1, 0.0, 200.0), (3.0, 0.0, 300.0), (3.2, 0.0, 30.0)],
+                   [1, 1, 1, 1, 0])
+    rec["turb_u"] = [0.8, -0.5, 0.4, -0.2, 0.0]
+    rec["turb_v"] = [-0.3, 1.1, 0.7, -0.4, 0.0]
+    rec["turb_w"] = [0.1, -0.2, -1.0, 0.6, 0.0]
+    ust, wst = [0.30, 0.25, 0.35, 0.28], [1.80, 0.0, 0.0, 1.60]
+    hmix, oli = [900.0, 800.0, 700.0, 1000.0], [-0.02, 0.0, 0.01, -0.0125]
+    pbl = api.Pbl(ctx, 4, 1)
+    pbl.upload(ust, wst, hmix, oli)
+    p = _upload(ctx, rec)
+    hanna = cbl.compute_hanna_params_gpu(ctx, p, pbl)
+    ref_h = orc.hanna_params_slots(rec, ust, wst, hmix, oli, 4, 1)
+    # np.isclose: the neutral cell's L = +inf on both sides
+    assert np.isclose(hanna.view(np.float32).reshape(5, 16)[:, :13], ref_h[:, :13], rtol=5e-5, atol=5e-5).all()
+    key, counter = (0xDECAFBAD, 0x12345678), (0xA5A50001, 0xFACEB00C, 7, 9)
+    nxt = cbl.update_particles_turbulence_langevin_gpu(ctx, p, hanna, 45.0, 2.5e-4, 0, 0.01, key, counter)
+    assert nxt == orc.counter_add(list(counter), 5)
+    o = orc.Pbl(4, 1)
+    o.ustar[:], o.wstar[:], o.hmix[:], o.oli[:] = ust, wst, hmix, oli
+    s = orc.State.from_records(rec)
+    prm = StepParams.production(turb_dt_seconds=45.0, rho_grad_over_rho=2.5e-4, key=key, counter=counter)
+    prm.stages, prm.n_substeps, prm.dry_mode, prm.wet_mode = 2, 0, 0, 0
+    flat = {k: np.zeros((4, 1, 2), np.float32) for k in ("u0", "v0", "w0", "u1", "v1", "w1")}
+    flat["heights"] = np.array([0.0, 1000.0], np.float32)             # no advection in this step
+    orc.step(s, 5, flat, o, prm)
+    got = p.download()
+    for f in ("turb_u", "turb_v", "turb_w"):
+        assert _close(got[f], getattr(s, f), 5e-5, 5e-5).all(), f
+    for f in ("pos_x", "pos_y", "pos_z", "cell_x", "cell_y", "flags", "cbt"):
+        assert np.array_equal(got[f], rec[f]), f                          # legacy: only the turbulence moves
+    assert np.all(got[4].tobytes() == rec[4].tobytes())
+
+
+def test_langevin_with_hanna_errors(ctx):
+    from flexpart_gpu import cbl
+    from flexpart_gpu._lib import FpgError
+    rec = _records([(0.5, 0.5, 10.0)] * 3)
+    p = _upload(ctx, rec)
+    with pytest.raises(FpgError) as e:                                 # MismatchedInputLengths
+        cbl.update_particles_turbulence_langevin_gpu(ctx, p, np.zeros(2, cbl.HANNA_PARAMS_DTYPE), 60.0, 0.0, 4,
+                                                     0.01, (1, 2), (0, 0, 0, 0))
+    assert e.value.status == -5
+    with pytest.raises(FpgError) as e:                                 # InvalidTimeStep
+        cbl.update_particles_turbulence_langevin_gpu(ctx, p, np.zeros(3, cbl.HANNA_PARAMS_DTYPE), 0.0, 0.0, 4,
+                                                     0.01, (1, 2), (0, 0, 0, 0))
+    assert e.value.status == -2
+    # zero records: sanitize_positive gives zero T_L, hence zero turbulence (langevin.wgsl:189-238)
+    nxt = cbl.update_particles_turbulence_langevin_gpu(ctx, p, np.zeros(3, cbl.HANNA_PARAMS_DTYPE), 60.0, 0.0, 0,
+                                                       0.01, (1, 2), (0, 0, 0, 0))
+    assert nxt == [3, 0, 0, 0]
+    got = p.download()
+    assert np.all(got["turb_u"] == 0) and np.all(got["turb_w"] == 0)
