@@ -57,10 +57,30 @@ UNIT = "particle-steps/s"
 BYTES_PER_PARTICLE_STEP = 96  # read 44 B + write 52 B of SoA state, one species
 SORT_EVERY = 12  # steps between spatial reorders (divides the default 24 timed steps after 4 warm-up)
 # DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
-# an ncu capture of a 2 M-particle launch (129.8 MB), scaled by the particle
+# an ncu capture of a 2 M-particle launch (135.1 MB), scaled by the particle
 # count; below the algorithmic 96 B because part of the state was still in
 # the 126 MB L2 across the capture's replay passes.
-DRAM_BYTES_PER_PARTICLE_NCU = 129.8e6 / 2.0e6
+DRAM_BYTES_PER_PARTICLE_NCU = 135.1e6 / 2.0e6
+# Warp instructions per 32 particle-steps of fused_step_kernel
+# (smsp__inst_executed.sum of the same capture: 176.8 M for 2 M particles).
+WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 176.8e6 / (2.0e6 / 32)
+
+
+def issue_roofline(n_particles, kernel_ms, clk):
+    """The fused step against the instruction-issue roofline: warp
+    instructions of one launch (the ncu count per 32 particle-steps, scaled by
+    the particles) over the kernel time, against 4 issues per clock on each
+    SM at the SM clock sampled during the timed region."""
+    import torch
+
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    instr = WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU * n_particles / 32.0
+    achieved = instr / (kernel_ms / 1e3)
+    peak = sms * 4 * mhz * 1e6
+    return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "instructions_per_launch": instr, "sm_mhz": mhz,
+            "source": "smsp__inst_executed.sum of a 2M-particle ncu capture, scaled by particles"}
 
 
 def parse():
@@ -826,7 +846,9 @@ def main():
                          "traffic_source": "ncu dram__bytes_read+write of a 2M-particle launch, scaled by particles",
                          "peak_kind": peak_kind,
                          "kernel": "fused_step_kernel", "kernel_ms": avg_kernel_ms,
-                         "bytes_per_launch": BYTES_PER_PARTICLE_STEP * n_active},
+                         "bytes_per_launch": BYTES_PER_PARTICLE_STEP * n_active,
+                         # the bound that binds: warp-instruction issue (148 SMs x 4 per clock)
+                         "issue": issue_roofline(n_active, avg_kernel_ms, clk)},
             "stages": stages,
             "clocks": clk,
             "gpu_launches": int(launches),
