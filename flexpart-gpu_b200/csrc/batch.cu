@@ -192,42 +192,52 @@ __global__ void __launch_bounds__(256) batch_grid_clear_kernel(const BatchState*
     }
 }
 
-// concentration_gridding.wgsl:323-345 per scenario, warp-aggregated as grid.cu.
+// concentration_gridding.wgsl:323-345 per scenario.  Each CTA bins a
+// contiguous range of tiles (a tile is 256 slots of one scenario); the key of
+// a particle is its index in the scenario-major grid, so one CTA table holds
+// the cells of every scenario its tiles touch.  Runs of equal keys in a warp
+// are summed by the segmented scan, the run ends add to the table, and the
+// table goes to the grids once per cell per CTA (grid_core.cuh).
 __global__ void __launch_bounds__(256) batch_grid_kernel(const BatchState* st, const ScenDev* __restrict__ sc,
                                                          const uint32_t* __restrict__ tile_scen, PopFields F,
-                                                         GridConst g, uint32_t* counts, uint32_t* mass) {
+                                                         GridConst g, uint32_t n_tiles, uint32_t tiles_per_cta,
+                                                         uint32_t* counts, uint32_t* mass) {
     if (g.every == 0 || (st->step + 1u) % g.every != 0u) return;
     __shared__ float s_h[FPG_MAX_LEVELS];
+    __shared__ uint32_t t_key[kTable], t_cnt[kTable], t_mass[kTable];
     for (uint32_t i = threadIdx.x; i < g.nz; i += blockDim.x) s_h[i] = g.h[i];
-    __syncthreads();
-    const uint32_t tile = blockIdx.x;
-    const uint32_t s = tile_scen[tile];
-    const ScenDev& d = sc[s];
-    const uint32_t local = (tile - d.first_tile) * TILE + threadIdx.x;
-    const uint32_t p = d.offset + local;
-    bool valid = local < d.released && (F.f[FPG_FIELD_FLAGS][p] & 1u);
-    uint32_t key = 0xffffffffu, q = 0u;
-    if (valid) {
-        const int32_t cx = (int32_t)F.f[FPG_FIELD_CELL_X][p], cy = (int32_t)F.f[FPG_FIELD_CELL_Y][p];
-        const uint32_t ix = (uint32_t)min(max(cx, 0), (int)g.nx - 1);
-        const uint32_t iy = (uint32_t)min(max(cy, 0), (int)g.ny - 1);
-        const uint32_t iz = level_of(__uint_as_float(F.f[FPG_FIELD_POS_Z][p]), s_h, g.nz, g.meters);
-        key = s * g.cells + (ix * g.ny + iy) * g.nz + iz;
-        q = quantize(fmaxf(__uint_as_float(F.f[FPG_FIELD_MASS0][p]), 0.0f), g.scale);
+    for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
+        t_key[i] = kEmpty;
+        t_cnt[i] = 0u;
+        t_mass[i] = 0u;
     }
+    __syncthreads();
     const unsigned lane = threadIdx.x & 31u;
-    unsigned pending = __ballot_sync(0xffffffffu, valid);
-    while (pending) {
-        const int src = __ffs(pending) - 1;
-        const uint32_t k = __shfl_sync(0xffffffffu, key, src);
-        const bool mine = valid && key == k;
-        const unsigned grp = __ballot_sync(0xffffffffu, mine);
-        const uint32_t qs = __reduce_add_sync(0xffffffffu, mine ? q : 0u);
-        if (lane == (unsigned)src) {
-            atomicAdd(counts + k, (uint32_t)__popc(grp));
-            atomicAdd(mass + k, qs);
+    const uint32_t t0 = blockIdx.x * tiles_per_cta;
+    const uint32_t t1 = min(t0 + tiles_per_cta, n_tiles);
+    for (uint32_t tile = t0; tile < t1; ++tile) {                       // uniform across the CTA
+        const uint32_t s = tile_scen[tile];
+        const ScenDev& d = sc[s];
+        const uint32_t local = (tile - d.first_tile) * TILE + threadIdx.x;
+        const uint32_t p = d.offset + local;
+        uint32_t key = kEmpty, q = 0u;
+        if (local < d.released && (F.f[FPG_FIELD_FLAGS][p] & 1u)) {
+            const int32_t cx = (int32_t)F.f[FPG_FIELD_CELL_X][p], cy = (int32_t)F.f[FPG_FIELD_CELL_Y][p];
+            const uint32_t ix = (uint32_t)min(max(cx, 0), (int)g.nx - 1);
+            const uint32_t iy = (uint32_t)min(max(cy, 0), (int)g.ny - 1);
+            const uint32_t iz = level_of(__uint_as_float(F.f[FPG_FIELD_POS_Z][p]), s_h, g.nz, g.meters);
+            key = s * g.cells + (ix * g.ny + iy) * g.nz + iz;
+            q = quantize(fmaxf(__uint_as_float(F.f[FPG_FIELD_MASS0][p]), 0.0f), g.scale);
         }
-        pending &= ~grp;
+        warp_runs_add(key, q, lane, t_key, t_cnt, t_mass, counts, mass);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
+        const uint32_t k = t_key[i];
+        if (k != kEmpty) {
+            atomicAdd(counts + k, t_cnt[i]);
+            atomicAdd(mass + k, t_mass[i]);
+        }
     }
 }
 
@@ -343,11 +353,15 @@ void enqueue_post(fpg_batch* b, cudaStream_t s) {
     const BatchConst c = make_const(b);
     const GridConst g = make_grid_const(b);
     const size_t total = (size_t)g.cells * b->scen.size();
-    if (g.every && g.cells) {
+    if (g.every && g.cells && b->n_tiles) {
         batch_grid_clear_kernel<<<b->ctx->sm_count * 4, 256, 0, s>>>(b->st, g.every, b->grid_counts, b->grid_mass,
                                                                      total);
-        batch_grid_kernel<<<b->n_tiles, 256, 0, s>>>(b->st, b->sc, b->tile_scen, pop_fields(b), g, b->grid_counts,
-                                                     b->grid_mass);
+        // 8 resident CTAs per SM, each over a contiguous range of tiles
+        const uint32_t ctas = std::max<uint32_t>(1u, std::min<uint32_t>(b->n_tiles, (uint32_t)b->ctx->sm_count * 8u));
+        const uint32_t per = (b->n_tiles + ctas - 1u) / ctas;
+        const uint32_t blocks = std::max<uint32_t>(1u, (b->n_tiles + per - 1u) / per);
+        batch_grid_kernel<<<blocks, 256, 0, s>>>(b->st, b->sc, b->tile_scen, pop_fields(b), g, b->n_tiles, per,
+                                                 b->grid_counts, b->grid_mass);
         b->ctx->count(2);
     }
     if (b->inv) enqueue_inverse_sample(b, s);

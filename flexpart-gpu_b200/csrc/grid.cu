@@ -37,56 +37,12 @@ __device__ __forceinline__ uint32_t cell_of(const GridArgs& a, const float* h, u
     return (ix * a.ny + iy) * a.nz + iz;
 }
 
-// The CTA's table of the cells its chunk touches: open addressing on the
-// cell index in shared memory, filled with shared atomics and added to the
-// global grid at the end, one pair of atomics per distinct cell per CTA.
-constexpr uint32_t kTableBits = 10;
-constexpr uint32_t kTable = 1u << kTableBits;             // 1024 entries
-constexpr uint32_t kProbes = 8;
-constexpr uint32_t kEmpty = 0xffffffffu;   // no cell has this index (cells < 2^32 - 1)
 constexpr uint32_t kSlotsPerThread = 2;
 
-__device__ __forceinline__ void table_add(uint32_t* tk, uint32_t* tc, uint32_t* tm, uint32_t k, uint32_t c,
-                                          uint32_t m, uint32_t* __restrict__ counts, uint32_t* __restrict__ mass) {
-    uint32_t slot = (k * 2654435761u) >> (32 - kTableBits);
-    for (uint32_t i = 0; i < kProbes; ++i) {
-        const uint32_t old = atomicCAS(tk + slot, kEmpty, k);
-        if (old == kEmpty || old == k) {
-            atomicAdd(tc + slot, c);
-            atomicAdd(tm + slot, m);
-            return;
-        }
-        slot = (slot + 1u) & (kTable - 1u);
-    }
-    atomicAdd(counts + k, c);               // crowded table: straight to the grid
-    atomicAdd(mass + k, m);
-}
-
-// Sums one warp's 32 (cell, scaled mass) pairs by runs of equal cells in
-// lane order: a run's last lane holds the run's count (its length) and mass
-// (a segmented inclusive scan, five shuffles) and adds them to the table.
-// The reorder leaves a warp's cells in a few runs; a cell that appears in
-// several runs is simply added several times.  Invalid lanes carry kEmpty
-// and add nothing.
-__device__ __forceinline__ void warp_runs_add(uint32_t key, uint32_t q, unsigned lane, uint32_t* tk, uint32_t* tc,
-                                              uint32_t* tm, uint32_t* __restrict__ counts,
-                                              uint32_t* __restrict__ mass) {
-    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const uint32_t next = __shfl_down_sync(0xffffffffu, key, 1);
-    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0u || prev != key);
-    const unsigned start = 31u - __clz(heads & (0xffffffffu >> (31u - lane)));
-    uint32_t v = q;
-#pragma unroll
-    for (unsigned d = 1; d < 32u; d <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, v, d);
-        if (lane >= start + d) v += x;
-    }
-    if ((lane == 31u || next != key) && key != kEmpty) table_add(tk, tc, tm, key, lane - start + 1u, v, counts, mass);
-}
-
 // Each CTA bins one contiguous chunk of slots, two slots per thread per
-// pass with every field loaded up front (four per pass measured no faster).  All sums are u32, so the grid
-// does not depend on the order of the additions.
+// pass with every field loaded up front (four per pass measured no
+// faster).  All sums are u32, so the grid does not depend on the order of
+// the additions.
 __global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, uint32_t chunk,
                                                    uint32_t* __restrict__ counts, uint32_t* __restrict__ mass) {
     __shared__ float s_h[FPG_MAX_LEVELS];
