@@ -103,3 +103,21 @@ def test_batch_tuning_candidates_listed_without_a_device():
     shapes = {(t["block_threads"], t["min_blocks_per_sm"], t["particles_per_thread"]) for t in c}
     assert (256, 4, 1) in shapes
     assert len(shapes) == len(c)
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """No CPU fallback: without libfpg.so the package does not import."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "try:\n"
+            "    import flexpart_gpu.api\n"
+            "except ImportError as e:\n"
+            "    print('refused:', e)\n"
+            "    sys.exit(0)\n"
+            "sys.exit(3)\n") % os.path.join(ROOT, "flexpart-gpu_b200")
+    env = dict(os.environ, FPG_LIBRARY=str(tmp_path / "absent" / "libfpg.so"))
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "no CPU fallback" in r.stdout
