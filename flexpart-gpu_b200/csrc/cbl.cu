@@ -100,6 +100,10 @@ __device__ __forceinline__ void store_zero_output(fpg_cbl_sampling_output* out, 
     o[0] = z; o[1] = z; o[2] = z;
 }
 
+// The kernels move records as 16-byte vectors: device pointers from the
+// caller must be 16-byte aligned (cudaMalloc gives 256).
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0u; }
+
 struct SlotView {
     const int32_t* cell_x;
     const int32_t* cell_y;
@@ -295,7 +299,7 @@ extern "C" fpg_status fpg_dispatch_hanna_params(fpg_ctx* ctx, const fpg_particle
     if (!ctx || !P || !pbl) return FPG_ERR_INVALID_ARGUMENT;
     if (P->dispatch == 0) return FPG_OK;
     if (n_out != P->dispatch) return FPG_ERR_LENGTH_MISMATCH;
-    if (!out_dev) return FPG_ERR_INVALID_ARGUMENT;
+    if (!out_dev || !aligned16(out_dev)) return FPG_ERR_INVALID_ARGUMENT;
     if (pbl->nx == 0 || pbl->ny == 0) return FPG_ERR_ZERO_SHAPE;
     if (pbl->nx > UINT32_MAX || pbl->ny > UINT32_MAX || P->dispatch > UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
     if (!pbl->ready) return FPG_ERR_NOT_READY;
@@ -317,6 +321,7 @@ extern "C" fpg_status fpg_cbl_sample(fpg_ctx* ctx, const fpg_particles* P, const
     if (n_hanna != v.n || n_inputs != v.n) return FPG_ERR_LENGTH_MISMATCH;
     if (v.n == 0) return FPG_OK;
     if (!hanna_dev || !inputs_dev || !out_dev) return FPG_ERR_INVALID_ARGUMENT;
+    if (!aligned16(hanna_dev) || !aligned16(inputs_dev) || !aligned16(out_dev)) return FPG_ERR_INVALID_ARGUMENT;
     if (v.n > UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
     cbl_sample_kernel<<<(unsigned)((v.n + 255) / 256), 256, 0, ctx->pick(stream)>>>(v, hanna_dev, inputs_dev,
                                                                                    out_dev);
@@ -334,7 +339,7 @@ extern "C" fpg_status fpg_cbl_sample_philox(fpg_ctx* ctx, const fpg_particles* P
     if (!pbl->ready) return FPG_ERR_NOT_READY;
     const SlotView v = slot_view(P);
     if (v.n == 0) return FPG_OK;
-    if (!out_dev) return FPG_ERR_INVALID_ARGUMENT;
+    if (!out_dev || !aligned16(out_dev)) return FPG_ERR_INVALID_ARGUMENT;
     const u32x4 c{counter[0], counter[1], counter[2], counter[3]};
     cbl_sample_philox_kernel<<<(unsigned)((v.n + 255) / 256), 256, 0, ctx->pick(stream)>>>(
         v, pbl->packed, (uint32_t)pbl->nx, (uint32_t)pbl->ny, key[0], key[1], c, out_dev);

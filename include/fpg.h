@@ -470,7 +470,9 @@ fpg_status fpg_philox_uniforms(fpg_ctx* ctx, const uint32_t key[2], const uint32
 /* ------------------------------------------------------------------------
  * Convective boundary layer and convective mixing
  * ---------------------------------------------------------------------- */
-/* HannaParams (src/pbl/mod.rs:23-57): 16 floats, 64 bytes per slot. */
+/* HannaParams (src/pbl/mod.rs:23-57): 16 floats, 64 bytes per slot.
+ * The record arrays below are read and written as 16-byte vectors: their
+ * device pointers must be 16-byte aligned (INVALID_ARGUMENT otherwise). */
 typedef struct fpg_hanna_params {
     float ust, wst, ol, h, zeta, sigu, sigv, sigw, dsigwdz, dsigw2dz, tlu, tlv, tlw;
     float pad[3];

@@ -385,3 +385,22 @@ def test_langevin_with_hanna_errors(ctx):
     assert nxt == [3, 0, 0, 0]
     got = p.download()
     assert np.all(got["turb_u"] == 0) and np.all(got["turb_w"] == 0)
+
+
+def test_record_pointers_must_be_16_byte_aligned(ctx):
+    """The CBL and Hanna kernels move records as 16-byte vectors; a
+    misaligned device pointer is refused before any launch."""
+    from flexpart_gpu import cbl
+    from flexpart_gpu._lib import lib
+    rec = _records([(0.5, 0.5, 10.0)] * 4)
+    p = _upload(ctx, rec)
+    pbl = api.Pbl(ctx, 1, 1)
+    pbl.upload([0.3], [1.0], [800.0], [-0.01])
+    buf = api.DeviceArray(ctx, 64 * 5, np.uint8)
+    off = api._vp(buf.ptr + 4)
+    assert lib.fpg_dispatch_hanna_params(ctx.h, p.h, pbl.h, off, 4, None) == -1
+    assert lib.fpg_cbl_sample(ctx.h, p.h, off, 4, api._vp(buf.ptr), 4, api._vp(buf.ptr), None) == -1
+    k, c = api._u32arr((1, 2), 2), api._u32arr((0, 0, 0, 0), 4)
+    assert lib.fpg_cbl_sample_philox(ctx.h, p.h, pbl.h, k, c, off, None) == -1
+    out = cbl.sample_cbl_vertical_velocity_philox(ctx, p, pbl, (1, 2), (0, 0, 0, 0))   # aligned: fine
+    assert out.size == 4
