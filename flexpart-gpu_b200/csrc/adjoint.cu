@@ -548,7 +548,10 @@ struct InverseData {
     float* bias = nullptr;
     bool has_bias = false;
     bool tape_in_forward = false;        // checkpoint_every == 0
-    uint32_t slices = 0;                 // tape slices: all steps, or the window length K
+    uint32_t slices = 0;                 // tape slices: all steps, or K x max(W, 1)
+    uint32_t window = 0;                 // K: steps per checkpoint window (all steps when taped)
+    uint32_t n_windows = 0;              // windows of the run (1 when taped)
+    uint32_t tail_windows = 0;           // W: last windows taped in the forward
     uint32_t n_ckpt = 0;
     uint32_t* ckpt = nullptr;            // n_ckpt * kNumCkptFields * capacity
     BatchState* ckpt_st = nullptr;
@@ -737,10 +740,17 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     d.nodes = nx * ny * nz;
     const size_t cells = nx * ny, cap = b->capacity;
     d.tape_in_forward = cfg->checkpoint_every == 0;
-    const uint32_t K = d.tape_in_forward ? (uint32_t)b->total_steps
-                                         : (uint32_t)std::min<uint64_t>(cfg->checkpoint_every, b->total_steps);
-    d.slices = K;
-    d.n_ckpt = d.tape_in_forward ? 0u : (uint32_t)((b->total_steps + K - 1) / K);
+    const uint32_t K = std::max<uint32_t>(1u, d.tape_in_forward
+                                                  ? (uint32_t)b->total_steps
+                                                  : (uint32_t)std::min<uint64_t>(cfg->checkpoint_every,
+                                                                                 b->total_steps));
+    d.window = K;
+    d.n_windows = d.tape_in_forward ? 1u : (uint32_t)((b->total_steps + K - 1) / K);
+    d.tail_windows = d.tape_in_forward ? 1u : std::min<uint32_t>(cfg->tape_tail_windows, d.n_windows);
+    // tail windows are taped in the forward, earlier ones recomputed into
+    // the same slices (step % slices) after the tail has been reversed
+    d.slices = d.tape_in_forward ? K : K * std::max<uint32_t>(d.tail_windows, 1u);
+    d.n_ckpt = d.tape_in_forward ? 0u : d.n_windows - d.tail_windows;
     // work items of 256 slots for the tape and adjoint kernels
     std::vector<uint2> items;
     for (size_t s = 0; s < n_src; ++s)
@@ -760,16 +770,17 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = alloc((void**)&d.ckpt, (size_t)d.n_ckpt * kNumCkptFields * cap * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.ckpt_st, std::max<uint32_t>(d.n_ckpt, 1) * sizeof(BatchState));
     if (e == cudaSuccess) e = alloc((void**)&d.ckpt_sc, (size_t)std::max<uint32_t>(d.n_ckpt, 1) * n_src * sizeof(ScenDev));
-    if (e == cudaSuccess) e = alloc((void**)&d.st_all, K * sizeof(BatchState));
-    if (e == cudaSuccess) e = alloc((void**)&d.sc_all, (size_t)K * n_src * sizeof(ScenDev));
-    if (e == cudaSuccess) e = alloc((void**)&d.tape, (size_t)K * TAPE_FIELDS * cap * 4);
+    const uint32_t S = d.slices;
+    if (e == cudaSuccess) e = alloc((void**)&d.st_all, S * sizeof(BatchState));
+    if (e == cudaSuccess) e = alloc((void**)&d.sc_all, (size_t)S * n_src * sizeof(ScenDev));
+    if (e == cudaSuccess) e = alloc((void**)&d.tape, (size_t)S * TAPE_FIELDS * cap * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.lam, (size_t)LAM_FIELDS * cap * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.dbias, d.nodes * 3 * 8);
     if (e == cudaSuccess) e = alloc((void**)&d.dbias_f, d.nodes * 3 * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.dsrc, n_src * 4 * 8);
     if (e == cudaSuccess) e = alloc((void**)&d.items, items.size() * sizeof(uint2));
     if (e == cudaSuccess) e = alloc((void**)&d.work, 4);
-    if (e == cudaSuccess) e = alloc((void**)&d.work_rev, (size_t)K * 4);
+    if (e == cudaSuccess) e = alloc((void**)&d.work_rev, (size_t)S * 4);
     cudaStream_t s = ctx->stream;
     if (e == cudaSuccess) e = cudaMemcpyAsync(d.rmap, rmap.data(), rmap.size() * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
@@ -860,11 +871,18 @@ extern "C" fpg_status fpg_inverse_forward(fpg_inverse* v, double* simulated) {
         }
     } else {
         if ((st = ensure_graph(b)) != FPG_OK) return st;
-        const uint32_t K = d.slices;
+        if (d.tail_windows && (st = ensure_tape_graph(v, 1)) != FPG_OK) return st;
+        const uint32_t K = d.window;
+        const uint64_t k_tail = (uint64_t)(d.n_windows - d.tail_windows) * K;
         for (uint64_t k = 0; k < b->total_steps; ++k) {
-            if (k % K == 0) FPG_CUDA(save_checkpoint(v, (uint32_t)(k / K)));
-            FPG_CUDA(cudaGraphLaunch(b->exec, s));
-            b->ctx->count(b->graph_launches);
+            if (k < k_tail) {
+                if (k % K == 0) FPG_CUDA(save_checkpoint(v, (uint32_t)(k / K)));
+                FPG_CUDA(cudaGraphLaunch(b->exec, s));
+                b->ctx->count(b->graph_launches);
+            } else {                         // a tail window: record its tape now
+                FPG_CUDA(cudaGraphLaunch(d.tape_exec[1], s));
+                b->ctx->count(d.tape_launches[1]);
+            }
         }
     }
     b->steps_done = b->total_steps;
@@ -900,13 +918,15 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
     const TapeBase tb = tape_base(v);
     const size_t smem = b->met->nz * sizeof(float);
     const uint64_t n = b->total_steps;
-    const uint32_t K = d.slices;
-    const int64_t windows = d.tape_in_forward ? 1 : (int64_t)d.n_ckpt;
+    const uint32_t K = d.window, S = d.slices;
+    const int64_t windows = d.n_windows;
+    // windows below this one are recomputed from their checkpoints
+    const int64_t first_taped = d.tape_in_forward ? 0 : (int64_t)(d.n_windows - d.tail_windows);
     fpg_status st = FPG_OK;
-    if (!d.tape_in_forward && (st = ensure_tape_graph(v, 0)) != FPG_OK) return st;
+    if (first_taped > 0 && (st = ensure_tape_graph(v, 0)) != FPG_OK) return st;
     for (int64_t w = windows - 1; w >= 0; --w) {
         const uint64_t k0 = (uint64_t)w * K, k1 = std::min<uint64_t>(k0 + K, n);
-        if (!d.tape_in_forward) {
+        if (w < first_taped) {
             // taped recompute of the window from its checkpoint; it leaves the
             // bracket of its last step packed
             FPG_CUDA(restore_checkpoint(v, (uint32_t)w));
@@ -916,11 +936,11 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
             }
             d.packed_ta = step_bracket_start(b, k1 - 1);
         }
-        // one work counter per slice of the window, cleared once
-        FPG_CUDA(cudaMemsetAsync(d.work_rev, 0, (size_t)K * 4, s));
+        // one work counter per slice, cleared once per window
+        FPG_CUDA(cudaMemsetAsync(d.work_rev, 0, (size_t)S * 4, s));
         // reverse of the window; the bracket is repacked only where it changes
         for (uint64_t k = k1; k-- > k0;) {
-            const uint32_t j = (uint32_t)(k % K);
+            const uint32_t j = (uint32_t)(k % S);
             const int64_t ta = step_bracket_start(b, k);
             if (ta != d.packed_ta) {
                 enqueue_pack_forced(b, d.st_all + j, s);
@@ -950,9 +970,10 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
             d_pos[3 * k + 2] = src[4 * k + 2];
         }
     }
-    // with checkpoints the population now holds the first window's
-    // recompute; the tape of a taped forward stays valid for another backward
-    if (!d.tape_in_forward) d.forward_done = false;
+    // after a recompute the population holds the first window's recompute
+    // and the tail slices are overwritten; a tape recorded entirely in the
+    // forward stays valid for another backward
+    if (first_taped > 0) d.forward_done = false;
     return FPG_OK;
 }
 

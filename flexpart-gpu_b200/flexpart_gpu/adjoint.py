@@ -32,6 +32,7 @@ def inversion_config(inv: synthetic.Inversion) -> InverseConfig:
     c.receptor_top_m = inv.receptor_top_m
     c.receptor_ramp_m = inv.receptor_ramp_m
     c.checkpoint_every = inv.checkpoint_every
+    c.tape_tail_windows = inv.tape_tail_windows
     return c
 
 

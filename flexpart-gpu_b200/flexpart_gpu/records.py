@@ -233,7 +233,7 @@ class InverseConfig(ctypes.Structure):
 
     _fields_ = [("batch", BatchConfig), ("sample_every_steps", ctypes.c_uint32),
                 ("receptor_top_m", ctypes.c_float), ("receptor_ramp_m", ctypes.c_float),
-                ("checkpoint_every", ctypes.c_uint32)]
+                ("checkpoint_every", ctypes.c_uint32), ("tape_tail_windows", ctypes.c_uint32)]
 
 
 class ReceptorRelease(ctypes.Structure):

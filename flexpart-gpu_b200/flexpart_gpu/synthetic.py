@@ -312,6 +312,7 @@ class Inversion:
     receptor_top_m: float = 100.0
     receptor_ramp_m: float = 20.0
     checkpoint_every: int = 8
+    tape_tail_windows: int = 0  # last windows taped in the forward (not recomputed)
 
 
 def config3(n_particles: int = 1_000_000, n_sources: int = 16, n_receptors: int = 200, hours: int = 24,

@@ -60,6 +60,10 @@ typedef struct fpg_inverse_config {
                                         steps/K checkpoints of 44 B per slot + K x 80 B per slot);
                                         0: the forward records the tape of every step (no recompute;
                                         steps x 80 B per slot) */
+    uint32_t tape_tail_windows;      /* with K >= 1: the forward also records the tape of its last
+                                        W windows (W x K x 80 B per slot, replacing their
+                                        checkpoints), which the backward reverses without
+                                        recomputing them; 0 = every window recomputed */
 } fpg_inverse_config;
 
 typedef struct fpg_inverse fpg_inverse;

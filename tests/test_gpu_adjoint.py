@@ -98,19 +98,22 @@ def test_gradient_does_not_depend_on_the_checkpoint_interval(ctx):
 
 
 def test_gradient_across_brackets_checkpoints_and_a_repeated_backward(ctx):
-    """7 h spans three met brackets, so the reverse sweep repacks the
-    bracket where it changes (and only there): the tape recorded in the
-    forward (K = 0), checkpoints every 2 and 5 steps, and a second backward
-    over the same tape give the same gradient."""
+    """7 h (29 steps) spans three met brackets, so the reverse sweep repacks
+    the bracket where it changes (and only there).  The tape recorded in the
+    forward (K = 0); checkpoints every 2 and 5 steps; the same with the last
+    3 / 2 windows taped in the forward instead of recomputed; every window
+    taped (W above the window count) — all give the same gradient, and a
+    second backward over a tape recorded entirely in the forward repeats it."""
     grads = []
-    for K in (0, 2, 5):
+    for K, W in ((0, 0), (2, 0), (5, 0), (2, 3), (5, 2), (4, 100)):
         inv = _problem(7, smooth=False, K=K)
+        inv.tape_tail_windows = W
         model = adj.SourceInversion(ctx, inv)
         sim = model.forward(model.mass0, model.position0)
         _, d = adj.misfit(sim, _obs(sim))
         grads.append(model.backward(d))
-        if K == 0:
-            _assert_same_gradient(model.backward(d), grads[0])
+        if K == 0 or W == 100:
+            _assert_same_gradient(model.backward(d), grads[-1])
         del model
     for g in grads[1:]:
         _assert_same_gradient(g, grads[0])
