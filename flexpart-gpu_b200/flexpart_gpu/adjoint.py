@@ -93,13 +93,21 @@ class SourceInversion:
         check(lib.fpg_inverse_forward(self.h, _p(sim)), "fpg_inverse_forward")
         return sim[: self.n_receptors]
 
-    def backward(self, d_sim, want_bias: bool = True):
+    def backward(self, d_sim, want_bias: bool = True, group=None):
+        """Gradients of the loss given dL/dsim.  With `group` (a
+        torch.distributed group whose ranks each hold a shard of the
+        instances), the wind-bias gradient is summed over the ranks in fixed
+        point (distributed.allreduce_gradient_fixed_point); the source
+        gradients stay per rank."""
         g = np.ascontiguousarray(d_sim, np.float64)
         dm = np.zeros(self.n_sources, np.float64)
         dp = np.zeros((self.n_sources, 3), np.float64)
         nx, ny, nz = self.shape
         db = np.zeros((nx, ny, nz, 3), np.float32) if want_bias else None
         check(lib.fpg_inverse_backward(self.h, _p(g), _p(dm), _p(dp), _p(db)), "fpg_inverse_backward")
+        if db is not None and group is not None:
+            from .distributed import allreduce_gradient_fixed_point
+            db = allreduce_gradient_fixed_point(db, group).astype(np.float32)
         return {"mass": dm, "position": dp, "wind_bias": db}
 
 

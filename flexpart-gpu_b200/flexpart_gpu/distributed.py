@@ -12,6 +12,11 @@ over the whole population, in any order.
 Philox streams of different ranks must not overlap: rank r uses the
 counter's top word r (the step advance only carries into it after 2^96
 blocks).
+
+An inversion whose instances are sharded across ranks exchanges one thing:
+the wind-bias gradient, shared by every instance, summed once per backward
+in fixed point (int64 at a common power-of-two scale) so that the sum does
+not depend on the reduction order.
 """
 from __future__ import annotations
 
@@ -81,4 +86,44 @@ def allreduce_grids_device(counts_ptr: int, mass_ptr: int, n: int, group=None):
         dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
 
 
-__all__ = ["shard_range", "shard_scenarios", "rank_counter", "allreduce_grids", "allreduce_grids_device"]
+def _fixed_point_exponent(max_abs: float, world: int, bits: int = 62) -> int:
+    """Power-of-two scale 2^e for the fixed-point sum: the largest e with
+    world * max_abs * 2^e <= 2^bits, so no partial sum overflows int64."""
+    if not (max_abs > 0.0) or not np.isfinite(max_abs):
+        return 0
+    return int(np.floor(np.log2(2.0 ** bits / (world * max_abs))))
+
+
+def fixed_point_sum(arrays, bits: int = 62) -> np.ndarray:
+    """The sum allreduce_gradient_fixed_point computes, in one process: each
+    array rounded to int64 at the common power-of-two scale, the integers
+    summed exactly, the total scaled back."""
+    arrays = [np.asarray(a, np.float64) for a in arrays]
+    e = _fixed_point_exponent(max(float(np.max(np.abs(a))) if a.size else 0.0 for a in arrays), len(arrays), bits)
+    q = sum(np.rint(np.ldexp(a, e)).astype(np.int64) for a in arrays)
+    return np.ldexp(q.astype(np.float64), -e)
+
+
+def allreduce_gradient_fixed_point(grad: np.ndarray, group=None, bits: int = 62) -> np.ndarray:
+    """Sum over ranks of a float gradient (the wind-bias gradient of an
+    inversion whose instances are sharded across ranks) in fixed point:
+    one MAX all-reduce fixes a common power-of-two scale, the rounded int64
+    values are summed exactly, so the result does not depend on the ranks'
+    reduction order and is bit-identical to fixed_point_sum of the ranks'
+    gradients.  Host arrays; CUDA tensors when the group's backend is NCCL."""
+    import torch
+    import torch.distributed as dist
+
+    g = np.asarray(grad, np.float64)
+    world = dist.get_world_size(group)
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    m = torch.tensor([float(np.max(np.abs(g))) if g.size else 0.0], dtype=torch.float64, device=dev)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX, group=group)
+    e = _fixed_point_exponent(float(m.item()), world, bits)
+    q = torch.from_numpy(np.rint(np.ldexp(g, e)).astype(np.int64)).to(dev)
+    dist.all_reduce(q, op=dist.ReduceOp.SUM, group=group)
+    return np.ldexp(q.cpu().numpy().astype(np.float64), -e).reshape(np.shape(grad))
+
+
+__all__ = ["shard_range", "shard_scenarios", "rank_counter", "allreduce_grids", "allreduce_grids_device",
+           "fixed_point_sum", "allreduce_gradient_fixed_point"]

@@ -132,3 +132,41 @@ def test_a_rank_that_leaves_is_detected_by_the_next_collective():
         if p.is_alive():
             p.kill()
     assert res.startswith("error"), res
+
+
+def _gradient_worker(rank, world, port, q):
+    dist = _init(rank, world, port)
+    try:
+        rng = np.random.default_rng(100 + rank)
+        g = rng.standard_normal(5000) * 10.0 ** rng.uniform(-6, 2, 5000)
+        s = fd.allreduce_gradient_fixed_point(g)
+        if rank == 0:
+            parts = [np.random.default_rng(100 + r) for r in range(world)]
+            arrays = [p.standard_normal(5000) * 10.0 ** p.uniform(-6, 2, 5000) for p in parts]
+            ref = fd.fixed_point_sum(arrays)
+            flipped = fd.fixed_point_sum(arrays[::-1])
+            exact = np.sum(np.array(arrays, np.float64), axis=0)
+            q.put((bool(np.array_equal(s, ref)), bool(np.array_equal(ref, flipped)),
+                   float(np.max(np.abs(s - exact)) / np.max(np.abs(exact)))))
+    except Exception as e:  # noqa: BLE001 - reported to the parent
+        q.put(("error", repr(e)))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+def test_wind_bias_gradient_sum_over_ranks_is_order_independent():
+    """The one exchange of an inversion sharded by instance: the wind-bias
+    gradient summed in fixed point equals the one-process fixed-point sum
+    bit for bit (in either rank order) and the float sum to ~1e-16."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gradient_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+    assert res[0] is True and res[1] is True, res
+    assert res[2] < 1e-15, res
