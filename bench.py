@@ -648,6 +648,10 @@ def main():
 
     # ---- device-resident met ring for the timed loop ----
     frame_dev = [tuple(api.DeviceArray.from_numpy(ctx, f[k].reshape(-1)) for k in ("u", "v", "w")) for f in frames]
+    # the surface frames and precipitation fields too: every input of the
+    # timed loop is resident in HBM before it starts
+    surf_dev = [api.DeviceArray.from_numpy(ctx, f["surface"].view(np.uint8)) for f in frames]
+    precip_dev = [api.DeviceArray.from_numpy(ctx, np.ascontiguousarray(p, np.float32).reshape(-1)) for p in precip]
     met = api.Met(ctx, spec.nx, spec.ny, spec.nz)
     met.set_level_heights(heights)
     surf = api.Surface(ctx, spec.nx, spec.ny)
@@ -662,16 +666,17 @@ def main():
             u, v, w = frame_dev[fi]
             api.check(lib.fpg_met_upload_frame_device(met.h, which, ctypes.c_void_p(u.ptr), ctypes.c_void_p(v.ptr),
                                                       ctypes.c_void_p(w.ptr), None), "met frame")
-        surf.upload(0, frames[fa]["surface"])
-        surf.upload(1, frames[fb]["surface"])
-        wet.from_precipitation(precip[fa], None, None, scn.wet_a, scn.wet_b)
+        for which, fi in ((0, fa), (1, fb)):
+            api.check(lib.fpg_surface_upload(surf.h, which, ctypes.c_void_p(surf_dev[fi].ptr), None), "surface")
+        api.check(lib.fpg_cellfield_from_precipitation(wet.h, ctypes.c_void_p(precip_dev[fa].ptr), None, None,
+                                                       scn.wet_a, scn.wet_b, None), "wet cells")
 
     ev = []
     n_out_cells = scn.out_shape[0] * scn.out_shape[1] * scn.out_shape[2]
     # torch's collectives run on its current stream: make that the library's stream
     torch.cuda.set_stream(stream)
 
-    stage_ev = {"reorder": [], "pbl": [], "grid": []}
+    stage_ev = {"bracket": [], "reorder": [], "pbl": [], "grid": []}
 
     def staged(name, record, fn):
         if not record:
@@ -688,7 +693,7 @@ def main():
         t = state["t"]
         fa, fb, ta, tb = synthetic.bracket_frames(scn, t)
         if state["bracket"] != (fa, fb, ta):
-            set_bracket(fa, fb)
+            staged("bracket", record, lambda: set_bracket(fa, fb))
             state["bracket"] = (fa, fb, ta)
         alpha = (t - ta) / float(tb - ta)
         if state["k"] % args.sort_every == 0:

@@ -267,8 +267,9 @@ extern "C" fpg_status fpg_surface_destroy(fpg_surface* s) {
 
 extern "C" fpg_status fpg_surface_upload(fpg_surface* s, int32_t which, const fpg_surface_cell* cells, void* stream) {
     if (!s || !cells || (which != 0 && which != 1)) return FPG_ERR_INVALID_ARGUMENT;
+    // host or device memory (the copy kind follows the pointer, unified addressing)
     FPG_CUDA(cudaMemcpyAsync(s->frame[which], cells, s->nx * s->ny * sizeof(fpg_surface_cell),
-                             cudaMemcpyHostToDevice, s->ctx->pick(stream)));
+                             cudaMemcpyDefault, s->ctx->pick(stream)));
     s->uploaded[which] = true;
     return FPG_OK;
 }
@@ -335,12 +336,13 @@ extern "C" fpg_status fpg_cellfield_from_precipitation(fpg_cellfield* f, const f
     float* d_lsp = f->staging;
     float* d_conv = f->staging + n;
     float* d_cc = f->staging + 2 * n;
-    if (lsp) FPG_CUDA(cudaMemcpyAsync(d_lsp, lsp, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    // host or device arrays (the copy kind follows the pointer, unified addressing)
+    if (lsp) FPG_CUDA(cudaMemcpyAsync(d_lsp, lsp, n * sizeof(float), cudaMemcpyDefault, s));
     else FPG_CUDA(cudaMemsetAsync(d_lsp, 0, n * sizeof(float), s));
-    if (convp) FPG_CUDA(cudaMemcpyAsync(d_conv, convp, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    if (convp) FPG_CUDA(cudaMemcpyAsync(d_conv, convp, n * sizeof(float), cudaMemcpyDefault, s));
     else FPG_CUDA(cudaMemsetAsync(d_conv, 0, n * sizeof(float), s));
     if (cloud_cover) {
-        FPG_CUDA(cudaMemcpyAsync(d_cc, cloud_cover, n * sizeof(float), cudaMemcpyHostToDevice, s));
+        FPG_CUDA(cudaMemcpyAsync(d_cc, cloud_cover, n * sizeof(float), cudaMemcpyDefault, s));
     } else {
         fill_kernel<<<blocks_for(n, 256), 256, 0, s>>>(d_cc, (uint32_t)n, 1.0f);  // cloud cover 1
         f->ctx->count();

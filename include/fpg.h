@@ -243,7 +243,8 @@ fpg_status fpg_surface_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_surface** 
 fpg_status fpg_surface_destroy(fpg_surface* s);
 /* SurfaceFieldBuffer::upload of one frame: `which` 0 = t0, 1 = t1.  The
  * device lerps the two frames (io/temporal.rs:122,417-420) inside
- * fpg_pbl_diagnostics, so a bracket is uploaded once, not every step. */
+ * fpg_pbl_diagnostics, so a bracket is uploaded once, not every step.
+ * `cells` may be host or device memory (unified addressing). */
 fpg_status fpg_surface_upload(fpg_surface* s, int32_t which, const fpg_surface_cell* cells,
                               void* stream);
 
@@ -267,9 +268,9 @@ fpg_status fpg_cellfield_upload(fpg_cellfield* f, const float* lambda, const flo
 /* Derives the per-cell wet forcing from precipitation on the device:
  * wet_precipitation_state (src/physics/wet_scavenging.rs:179-207) gives the
  * precipitating fraction and sub-grid rate, then the below-cloud gas
- * coefficient a * prec^b (wet_scavenging.rs:213-225).  Inputs are host
- * arrays of large-scale and convective precipitation [mm/h] and cloud cover
- * [-] (any may be NULL = 0, cloud cover NULL = 1). */
+ * coefficient a * prec^b (wet_scavenging.rs:213-225).  Inputs are host or
+ * device arrays of large-scale and convective precipitation [mm/h] and
+ * cloud cover [-] (any may be NULL = 0, cloud cover NULL = 1). */
 fpg_status fpg_cellfield_from_precipitation(fpg_cellfield* f, const float* lsp_mm_h,
                                             const float* convp_mm_h, const float* cloud_cover,
                                             float gas_coefficient_a, float gas_exponent_b,
