@@ -258,3 +258,37 @@ def test_error_codes_mirror_reference(ctx):
     assert e.value.status == -7          # InvalidMassScale
     # the failed calls left the particles untouched
     assert np.array_equal(p.download(), rec)
+
+
+def test_surface_and_precipitation_accept_device_arrays(ctx):
+    """A caller whose met is already in HBM passes device pointers for the
+    surface frames and the precipitation: the PBL, and a step with the
+    per-cell wet forcing, come out bit for bit as from host arrays."""
+    import ctypes
+
+    spec, frames, met = small_met(seed=3)
+    lib = api._lib.lib
+    n = spec.nx * spec.ny
+    rng = np.random.default_rng(4)
+    lsp = np.where(rng.random(n) < 0.3, rng.lognormal(-1, 1, n), 0).astype(np.float32)
+    rec = population(spec.nx, spec.ny, 3000, seed=12)
+    out = {}
+    for label in ("host", "device"):
+        m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.3, rec)
+        cf = api.CellField(ctx, spec.nx, spec.ny)
+        if label == "host":
+            cf.from_precipitation(lsp, None, None, 1e-4, 0.8)
+        else:
+            keep = [api.DeviceArray.from_numpy(ctx, frames[k]["surface"].view(np.uint8)) for k in (0, 1)]
+            d_lsp = api.DeviceArray.from_numpy(ctx, lsp)
+            for k in (0, 1):
+                surf.upload(k, np.zeros_like(frames[k]["surface"]))       # overwritten by the device copy
+                api.check(lib.fpg_surface_upload(surf.h, k, ctypes.c_void_p(keep[k].ptr), None), "surface")
+            api.check(lib.fpg_cellfield_from_precipitation(cf.h, ctypes.c_void_p(d_lsp.ptr), None, None, 1e-4, 0.8,
+                                                           None), "wet cells")
+            api.pbl_diagnostics(ctx, surf, 0.3, pbl)
+        api.step(ctx, p, m, pbl, production_params(alpha=0.3, wet_mode=3), wet_cells=cf)
+        out[label] = (pbl.download(), p.download().tobytes())
+    for k in ("ustar", "wstar", "hmix", "oli", "sshf", "ssr", "surfstr"):
+        assert out["host"][0][k].tobytes() == out["device"][0][k].tobytes(), k
+    assert out["host"][1] == out["device"][1]
