@@ -404,3 +404,28 @@ def test_record_pointers_must_be_16_byte_aligned(ctx):
     assert lib.fpg_cbl_sample_philox(ctx.h, p.h, pbl.h, k, c, off, None) == -1
     out = cbl.sample_cbl_vertical_velocity_philox(ctx, p, pbl, (1, 2), (0, 0, 0, 0))   # aligned: fine
     assert out.size == 4
+
+
+def test_edge_sizes(ctx):
+    """One convection level; an empty dispatch for every entry point."""
+    from flexpart_gpu import cbl
+    from flexpart_gpu import convection as cv
+    rec = _records([(0.5, 0.5, -20.0), (0.5, 0.5, 300.0), (0.5, 0.5, 5000.0)], [1, 1, 0])
+    p = _upload(ctx, rec)
+    cm = cv.ConvectiveMixing(ctx, 1)
+    cm.set_matrix(np.ones(1, np.float32), [0.0, 1000.0])
+    cm.apply(p)
+    got = p.download()
+    assert got["pos_z"].tolist() == [500.0, 500.0, 5000.0] and got["cbt"].tolist() == [0, 0, 0]
+    assert got.tobytes() == orc.convective_mixing(rec, np.ones(1, np.float32), [0.0, 1000.0]).tobytes()
+    empty = api.Particles(ctx, 4)
+    empty.dispatch_count = 0
+    cm.apply(empty)
+    pbl = api.Pbl(ctx, 1, 1)
+    pbl.upload([0.3], [1.0], [800.0], [-0.01])
+    assert cbl.compute_hanna_params_gpu(ctx, empty, pbl).size == 0
+    assert cbl.sample_cbl_vertical_velocity_philox(ctx, empty, pbl, (1, 2), (0, 0, 0, 0)).size == 0
+    assert cbl.sample_cbl_vertical_velocity_gpu(ctx, empty, np.zeros(0, cbl.HANNA_PARAMS_DTYPE),
+                                                np.zeros(0, cbl.CBL_INPUT_DTYPE)).size == 0
+    assert cbl.update_particles_turbulence_langevin_gpu(ctx, empty, np.zeros(0, cbl.HANNA_PARAMS_DTYPE), 60.0, 0.0,
+                                                        4, 0.01, (1, 2), (5, 0, 0, 0)) == [5, 0, 0, 0]
