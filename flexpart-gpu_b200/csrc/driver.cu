@@ -15,7 +15,12 @@
 // so every particle draws the same Philox blocks as in the reference.
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -108,7 +113,39 @@ struct fpg_forward {
     std::vector<MetSlot> ring;
     cudaStream_t copy_stream = nullptr;
     uint64_t tick = 0, ring_hits = 0, host_uploads = 0;
+    // per-section timing (fpg_forward_set_profiling / FLEXPART_GPU_PROFILE=1)
+    bool profile = false, print_profile = false, have_timing = false;
+    cudaEvent_t marks[7] = {};
+    fpg_step_timing last_timing{};
 };
+
+namespace {
+
+// One NVTX range (a named span in Nsight timelines; nothing without a tool).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { end(); }
+    void end() {
+        if (open) nvtxRangePop();
+        open = false;
+    }
+    bool open = true;
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// Records section boundary k on the step stream when timing is on.
+void mark(fpg_forward* d, int k) {
+    if (d->profile) cudaEventRecord(d->marks[k], d->ctx->stream);
+}
+
+fpg_status ensure_marks(fpg_forward* d) {
+    for (cudaEvent_t& e : d->marks)
+        if (!e) FPG_CUDA(cudaEventCreate(&e));
+    return FPG_OK;
+}
+
+}  // namespace
 
 using namespace fpg;
 
@@ -166,7 +203,26 @@ extern "C" fpg_status fpg_forward_destroy(fpg_forward* d) {
         cudaStreamSynchronize(d->copy_stream);
         cudaStreamDestroy(d->copy_stream);
     }
+    for (cudaEvent_t e : d->marks)
+        if (e) cudaEventDestroy(e);
     delete d;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_set_profiling(fpg_forward* d, int32_t on) {
+    if (!d) return FPG_ERR_INVALID_ARGUMENT;
+    if (on) {
+        const fpg_status st = ensure_marks(d);
+        if (st != FPG_OK) return st;
+    }
+    d->profile = on != 0;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_last_timing(const fpg_forward* d, fpg_step_timing* out) {
+    if (!d || !out) return FPG_ERR_INVALID_ARGUMENT;
+    if (!d->have_timing) return FPG_ERR_NOT_READY;
+    *out = d->last_timing;
     return FPG_OK;
 }
 
@@ -214,6 +270,12 @@ static fpg_status driver_create(fpg_ctx* ctx, const fpg_forward_config* cfg, con
     if (st == FPG_OK) st = fpg_pbl_create(ctx, nx, ny, &d->pbl);
     if (st == FPG_OK && cfg->use_compaction) st = fpg_compaction_create(ctx, capacity, &d->compaction);
     if (st == FPG_OK && cfg->sort_interval_steps) st = fpg_sorter_create(ctx, capacity, &d->sorter);
+    // is_profiling_enabled (timeloop.rs:469-476)
+    const char* prof = std::getenv("FLEXPART_GPU_PROFILE");
+    if (st == FPG_OK && prof && std::strcmp(prof, "1") == 0) {
+        st = fpg_forward_set_profiling(d, 1);
+        d->print_profile = true;
+    }
     if (st != FPG_OK) {
         fpg_forward_destroy(d);
         return st;
@@ -324,19 +386,29 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
     if (!d || !met || !f) return FPG_ERR_INVALID_ARGUMENT;
     if (!fpg_forward_has_remaining_steps(d)) return FPG_ERR_SIMULATION_COMPLETE;
     fpg_status st;
+    const auto host_t0 = std::chrono::steady_clock::now();
+    NvtxRange step_range("fpg step");
+    mark(d, 0);
 
     // apply_spatial_sort_if_enabled (timeloop.rs:1414-1430)
     if (d->sorter && d->step_index % d->cfg.sort_interval_steps == 0 && d->next_free > 0) {
+        NvtxRange r("reorder");
         const size_t keep = d->particles->dispatch;
         d->particles->dispatch = d->next_free;
         st = fpg_sort_by_cell(d->ctx, d->particles, d->met, d->sorter, nullptr, nullptr);
         d->particles->dispatch = keep;
         if (st != FPG_OK) return st;
     }
+    mark(d, 1);
 
     uint64_t released = 0, first_slot = 0;
-    st = release_for_time(d, d->t, released, first_slot);
+    {
+        NvtxRange r("release");
+        st = release_for_time(d, d->t, released, first_slot);
+    }
     if (st != FPG_OK) return st;
+    mark(d, 2);
+    NvtxRange bracket_range("met bracket");
 
     // interpolation_alpha (timeloop.rs:2086-2120)
     const int64_t t0 = met->time_t0_seconds, t1 = met->time_t1_seconds;
@@ -372,8 +444,15 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
         d->bracket_t0 = t0;
         d->bracket_t1 = t1;
     }
+    bracket_range.end();
+    mark(d, 3);
     // interpolate_surface_fields_linear + encode_pbl_diagnostics (timeloop.rs:961-988,1079-1088)
-    if ((st = fpg_pbl_diagnostics(d->ctx, d->surface, alpha, &d->cfg.pbl_options, d->pbl, nullptr))) return st;
+    {
+        NvtxRange r("pbl");
+        if ((st = fpg_pbl_diagnostics(d->ctx, d->surface, alpha, &d->cfg.pbl_options, d->pbl, nullptr))) return st;
+    }
+    mark(d, 4);
+    NvtxRange step_kernel_range("fused step");
 
     // the fused step (timeloop.rs:1095-1180)
     const float dt = (float)d->cfg.timestep_seconds;
@@ -440,8 +519,11 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
         d->counter[3] = d->counter[3] + carry2;
     }
 
+    step_kernel_range.end();
+    mark(d, 5);
     // compaction (timeloop.rs:1185-1197,1249-1262)
     if (d->compaction) {
+        NvtxRange r("compaction");
         uint32_t act = 0;
         d->particles->dispatch = d->capacity;
         if ((st = fpg_compact(d->ctx, d->particles, d->compaction, &act, nullptr, nullptr))) return st;
@@ -458,6 +540,35 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
         report->first_released_slot = first_slot;
         report->active_particle_count = d->active;
         std::memcpy(report->next_philox_counter, d->counter, sizeof(d->counter));
+    }
+    mark(d, 6);
+    if (d->profile) {
+        // StepTimingReport (timeloop.rs:398-467): device sections from the events
+        const double host_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host_t0).count();
+        FPG_CUDA(cudaEventSynchronize(d->marks[6]));
+        double sec[6];
+        for (int k = 0; k < 6; ++k) {
+            float ms = 0.0f;
+            FPG_CUDA(cudaEventElapsedTime(&ms, d->marks[k], d->marks[k + 1]));
+            sec[k] = ms;
+        }
+        float total = 0.0f;
+        FPG_CUDA(cudaEventElapsedTime(&total, d->marks[0], d->marks[6]));
+        fpg_step_timing& t = d->last_timing;
+        t.step_index = d->step_index;
+        t.sort_ms = sec[0]; t.release_ms = sec[1]; t.met_bracket_ms = sec[2];
+        t.pbl_ms = sec[3]; t.step_ms = sec[4]; t.compaction_ms = sec[5];
+        t.gpu_total_ms = total;
+        t.host_call_ms = host_ms;
+        t.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host_t0).count();
+        d->have_timing = true;
+        if (d->print_profile)
+            std::fprintf(stderr,
+                         "[profile] step=%llu reorder=%.3fms release=%.3fms met_bracket=%.3fms pbl=%.3fms "
+                         "step=%.3fms compaction=%.3fms gpu=%.3fms host_call=%.3fms total=%.3fms\n",
+                         (unsigned long long)t.step_index, t.sort_ms, t.release_ms, t.met_bracket_ms, t.pbl_ms,
+                         t.step_ms, t.compaction_ms, t.gpu_total_ms, t.host_call_ms, t.wall_ms);
     }
     d->step_index += 1;
     d->t += d->direction > 0 ? d->cfg.timestep_seconds : -d->cfg.timestep_seconds;

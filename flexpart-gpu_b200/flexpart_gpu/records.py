@@ -307,6 +307,18 @@ class StepReport(ctypes.Structure):
     ]
 
 
+class StepTiming(ctypes.Structure):
+    """``fpg_step_timing``: the per-section timing of one forward step, the
+    device form of StepTimingReport (timeloop.rs:398-467), in ms."""
+
+    _fields_ = [
+        ("step_index", ctypes.c_uint64), ("sort_ms", ctypes.c_double), ("release_ms", ctypes.c_double),
+        ("met_bracket_ms", ctypes.c_double), ("pbl_ms", ctypes.c_double), ("step_ms", ctypes.c_double),
+        ("compaction_ms", ctypes.c_double), ("gpu_total_ms", ctypes.c_double),
+        ("host_call_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
+    ]
+
+
 class ConvectionInputs(ctypes.Structure):
     """fpg_convection_inputs: SimplifiedEmanuelInputs (physics/convection.rs:68-82)."""
     _fields_ = [

@@ -28,6 +28,7 @@ from .records import (
     SourceCollection,
     SourceRegion,
     StepReport,
+    StepTiming,
 )
 
 _vp = ctypes.c_void_p
@@ -113,6 +114,17 @@ class ForwardDriver:
         check(lib.fpg_forward_met_ring_stats(self.h, ctypes.byref(hits), ctypes.byref(uploads)),
               "fpg_forward_met_ring_stats")
         return int(hits.value), int(uploads.value)
+
+    def set_profiling(self, on: bool = True):
+        """Per-section device timing of every step (each step then waits for
+        its device work); also on when FLEXPART_GPU_PROFILE=1 at creation."""
+        check(lib.fpg_forward_set_profiling(self.h, 1 if on else 0), "fpg_forward_set_profiling")
+
+    def last_timing(self) -> StepTiming:
+        """The timing of the last step run with profiling on."""
+        t = StepTiming()
+        check(lib.fpg_forward_last_timing(self.h, ctypes.byref(t)), "fpg_forward_last_timing")
+        return t
 
     def accumulate_concentration_grid(self, grid: Grid, species=0, mass_scale=1.0e6, outheights=None):
         oh = None if outheights is None else np.ascontiguousarray(outheights, np.float32)

@@ -153,6 +153,33 @@ fpg_status fpg_forward_prefetch_frame(fpg_forward* d, int64_t time_seconds, cons
 /* Brackets served from the ring and from host pointers so far. */
 fpg_status fpg_forward_met_ring_stats(const fpg_forward* d, uint64_t* ring_hits, uint64_t* host_uploads);
 
+/* Per-section timing of one run_timestep: the reference's StepTimingReport
+ * (timeloop.rs:398-467), measured here with CUDA events between the
+ * sections on the device (ms) plus the host's time inside the call.
+ * Sections: reorder, release (new particles uploaded), met bracket (ring
+ * repack or host upload), PBL diagnostics, the fused step, compaction. */
+typedef struct fpg_step_timing {
+    uint64_t step_index;
+    double sort_ms;
+    double release_ms;
+    double met_bracket_ms;
+    double pbl_ms;
+    double step_ms;
+    double compaction_ms;
+    double gpu_total_ms;           /* first to last section on the device */
+    double host_call_ms;           /* host time inside run_timestep before the wait */
+    double wall_ms;                /* host time of the call including the wait for the device */
+} fpg_step_timing;
+
+/* Turns the timing on or off (is_profiling_enabled, timeloop.rs:469-476:
+ * also on when FLEXPART_GPU_PROFILE=1 at create time, which in addition
+ * prints one summary line per step to stderr, as the reference does).
+ * With timing on, every run_timestep waits for its device work to finish.
+ * NVTX ranges mark every step and section whether timing is on or not. */
+fpg_status fpg_forward_set_profiling(fpg_forward* d, int32_t on);
+/* The timing of the last run_timestep made with timing on; NOT_READY if none. */
+fpg_status fpg_forward_last_timing(const fpg_forward* d, fpg_step_timing* out);
+
 /* ------------------------------------------------------------------------
  * Backward (receptor) mode: BackwardTimeLoopDriver
  * (src/simulation/timeloop.rs:1433-1909).

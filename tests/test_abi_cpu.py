@@ -61,7 +61,7 @@ def test_record_layouts_match_the_c_header(tmp_path):
         "fpg_source_collection": R.SourceCollection, "fpg_backward_config": R.BackwardConfig,
         "fpg_inverse_config": R.InverseConfig,
         "fpg_batch_config": R.BatchConfig, "fpg_convection_inputs": R.ConvectionInputs,
-        "fpg_convection_column": R.ConvectionColumn,
+        "fpg_convection_column": R.ConvectionColumn, "fpg_step_timing": R.StepTiming,
     }
     dtypes = {"fpg_hanna_params": R.HANNA_PARAMS_DTYPE, "fpg_cbl_sampling_input": R.CBL_INPUT_DTYPE,
               "fpg_cbl_sampling_output": R.CBL_OUTPUT_DTYPE, "fpg_particle": R.PARTICLE_DTYPE,

@@ -202,3 +202,69 @@ def test_device_grid_written_as_netcdf_snapshot(ctx, tmp_path):
         assert np.array_equal(f.variables["concentration_mass_kg"][:].reshape(-1), kg)
         assert f.variables["time"][0] == scn.end
     assert counts.sum() == 20_000
+
+
+_SECTIONS = ("sort_ms", "release_ms", "met_bracket_ms", "pbl_ms", "step_ms", "compaction_ms")
+
+
+def test_step_timing_sections_and_identical_results(ctx):
+    """Per-section timing (StepTimingReport, timeloop.rs:398-467): the sections
+    are non-negative and add up to the device total, the fused step takes
+    time, and turning the timing on changes no result."""
+    scn = _small(particles=20_000, hours=2)
+    frames = synthetic.make_frames(scn.met)
+    forcing = tl.uniform_forcing(dry_velocity=0.002)
+    finals = []
+    for profile in (False, True):
+        drv = _driver(ctx, scn, use_compaction=1, sort_interval_steps=3)
+        src = tl.BracketSource(scn, frames)
+        if profile:
+            drv.set_profiling(True)
+        with pytest.raises(api._lib.FpgError) as e:
+            drv.last_timing()
+        assert e.value.status == -11     # NotReady: no step timed yet
+        while drv.has_remaining_steps:
+            rep = drv.run_timestep(src.at(drv.current_time_seconds), forcing)
+            if not profile:
+                continue
+            t = drv.last_timing()
+            secs = [getattr(t, name) for name in _SECTIONS]
+            assert t.step_index == rep.step_index
+            assert min(secs) >= 0.0 and t.step_ms > 0.0
+            assert abs(sum(secs) - t.gpu_total_ms) <= 0.01 + 1e-3 * t.gpu_total_ms
+            assert t.wall_ms >= t.host_call_ms >= 0.0
+        finals.append(drv.particles.download())
+    assert finals[0].tobytes() == finals[1].tobytes()
+
+
+def test_profile_environment_variable_prints_one_line_per_step(tmp_path):
+    """FLEXPART_GPU_PROFILE=1 at creation prints a [profile] line per step to
+    stderr (is_profiling_enabled / print_summary, timeloop.rs:436-476)."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = tmp_path / "run.py"
+    script.write_text(
+        "from flexpart_gpu import api, synthetic, timeloop as tl\n"
+        "scn = synthetic.config0()\n"
+        "scn.sources[0].particle_count = 2000\nscn.capacity = 2000\nscn.end = scn.start + 3600\n"
+        "frames = synthetic.make_frames(scn.met)\n"
+        "ctx = api.Context(0)\n"
+        "drv = tl.ForwardDriver(ctx, tl.scenario_config(scn), tl.scenario_releases(scn), tl.scenario_domain(scn),\n"
+        "                       scn.capacity, (scn.met.nx, scn.met.ny, scn.met.nz))\n"
+        "src = tl.BracketSource(scn, frames)\n"
+        "n = 0\n"
+        "while drv.has_remaining_steps:\n"
+        "    drv.run_timestep(src.at(drv.current_time_seconds), tl.uniform_forcing())\n"
+        "    n += 1\n"
+        "print('steps', n)\n")
+    env = dict(os.environ, FLEXPART_GPU_PROFILE="1",
+               PYTHONPATH=os.pathsep.join([root, os.path.join(root, "flexpart-gpu_b200")]))
+    r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    steps = int(r.stdout.split()[-1])
+    lines = [ln for ln in r.stderr.splitlines() if ln.startswith("[profile] step=")]
+    assert steps > 0 and len(lines) == steps
+    assert all("step=" in ln and "gpu=" in ln and "total=" in ln for ln in lines)
