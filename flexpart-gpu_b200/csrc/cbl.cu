@@ -1,7 +1,7 @@
-// cbl.cu — convective-boundary-layer sampling and convective mixing:
+// cbl.cu — convective-boundary-layer sampling and convective mixing
+// (the per-slot Hanna records they read come from fpg_dispatch_hanna_params,
+// built with the step in step.cu):
 //
-// * fpg_dispatch_hanna_params: per-slot Hanna turbulence parameters from the PBL
-//   fields at the particle's cell (hanna_params.wgsl, src/gpu/hanna.rs);
 // * fpg_cbl_sample: the bi-Gaussian vertical-velocity PDF of the CBL and one
 //   sampled w' per slot from caller uniforms (cbl.wgsl, src/gpu/cbl.rs);
 // * fpg_cbl_sample_philox: the same sample fused with the Hanna sigma_w at
@@ -25,6 +25,7 @@
 
 #include "fpg_internal.h"
 #include "physics.cuh"
+#include "slots.cuh"
 
 namespace fpg {
 namespace {
@@ -98,63 +99,6 @@ __device__ __forceinline__ void store_zero_output(fpg_cbl_sampling_output* out, 
     float4* o = reinterpret_cast<float4*>(out + i);
     const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     o[0] = z; o[1] = z; o[2] = z;
-}
-
-// The kernels move records as 16-byte vectors: device pointers from the
-// caller must be 16-byte aligned (cudaMalloc gives 256).
-inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0u; }
-
-struct SlotView {
-    const int32_t* cell_x;
-    const int32_t* cell_y;
-    const float* pos_x;
-    const float* pos_y;
-    const float* pos_z;
-    const uint32_t* flags;
-    size_t n;
-};
-
-SlotView slot_view(const fpg_particles* P) {
-    return SlotView{static_cast<const int32_t*>(P->field[FPG_FIELD_CELL_X]),
-                    static_cast<const int32_t*>(P->field[FPG_FIELD_CELL_Y]),
-                    static_cast<const float*>(P->field[FPG_FIELD_POS_X]),
-                    static_cast<const float*>(P->field[FPG_FIELD_POS_Y]),
-                    static_cast<const float*>(P->field[FPG_FIELD_POS_Z]),
-                    static_cast<const uint32_t*>(P->field[FPG_FIELD_FLAGS]), P->dispatch};
-}
-
-// hanna_params.wgsl:244-250: the PBL cell of the particle's position.
-__device__ __forceinline__ float4 pbl_cell(const SlotView& v, size_t p, const float4* pbl, uint32_t pnx,
-                                           uint32_t pny) {
-    const float x = (float)v.cell_x[p] + v.pos_x[p];
-    const float y = (float)v.cell_y[p] + v.pos_y[p];
-    const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(pnx - 1u)));
-    const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(pny - 1u)));
-    return __ldg(pbl + (i * pny + j));
-}
-
-// hanna_params.wgsl:231-258 with compute_hanna (physics/hanna.rs:49-163):
-// one 64-byte HannaParams record per slot, zeros for inactive slots.
-__global__ void __launch_bounds__(256) hanna_params_kernel(SlotView v, const float4* __restrict__ pbl, uint32_t pnx,
-                                                           uint32_t pny, fpg_hanna_params* __restrict__ out) {
-    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= v.n) return;
-    float4* o = reinterpret_cast<float4*>(out + p);
-    if ((v.flags[p] & FLAG_ACTIVE) == 0u) {
-        const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        o[0] = z; o[1] = z; o[2] = z; o[3] = z;
-        return;
-    }
-    const float4 cell = pbl_cell(v, p, pbl, pnx, pny);
-    const float ol = obukhov_from_inverse(cell.w);
-    const float z = v.pos_z[p];
-    const Hanna hn = compute_hanna(cell.x, cell.y, ol, cell.z, z);
-    // zeta and d(sigma_w^2)/dz as the CPU routine forms them (hanna.rs:55,145)
-    const float zeta = clampf(clampf(z, 0.0f, hn.h) / hn.h, 0.0f, 1.0f);
-    o[0] = make_float4(hn.ust, hn.wst, hn.ol, hn.h);
-    o[1] = make_float4(zeta, hn.sigu, hn.sigv, hn.sigw);
-    o[2] = make_float4(hn.dsigwdz, 2.0f * hn.sigw * hn.dsigwdz, hn.tlu, hn.tlv);
-    o[3] = make_float4(hn.tlw, 0.0f, 0.0f, 0.0f);
 }
 
 // cbl.wgsl:251-298: PDF from the slot's Hanna record, sample from its uniforms.
@@ -293,24 +237,6 @@ struct fpg_convection {
     bool sorted = true;
     bool ready = false;
 };
-
-extern "C" fpg_status fpg_dispatch_hanna_params(fpg_ctx* ctx, const fpg_particles* P, const fpg_pbl* pbl,
-                                                fpg_hanna_params* out_dev, size_t n_out, void* stream) {
-    if (!ctx || !P || !pbl) return FPG_ERR_INVALID_ARGUMENT;
-    if (P->dispatch == 0) return FPG_OK;
-    if (n_out != P->dispatch) return FPG_ERR_LENGTH_MISMATCH;
-    if (!out_dev || !aligned16(out_dev)) return FPG_ERR_INVALID_ARGUMENT;
-    if (pbl->nx == 0 || pbl->ny == 0) return FPG_ERR_ZERO_SHAPE;
-    if (pbl->nx > UINT32_MAX || pbl->ny > UINT32_MAX || P->dispatch > UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
-    if (!pbl->ready) return FPG_ERR_NOT_READY;
-    const SlotView v = slot_view(P);
-    if (v.n == 0) return FPG_OK;
-    hanna_params_kernel<<<(unsigned)((v.n + 255) / 256), 256, 0, ctx->pick(stream)>>>(
-        v, pbl->packed, (uint32_t)pbl->nx, (uint32_t)pbl->ny, out_dev);
-    ctx->count();
-    FPG_CHECK_LAUNCH();
-    return FPG_OK;
-}
 
 extern "C" fpg_status fpg_cbl_sample(fpg_ctx* ctx, const fpg_particles* P, const fpg_hanna_params* hanna_dev,
                                      size_t n_hanna, const fpg_cbl_sampling_input* inputs_dev, size_t n_inputs,

@@ -23,6 +23,10 @@
 // Level heights sit in shared memory; the metres->level search is a binary
 // search when heights are non-decreasing (same first index as the
 // reference's linear scan, advection_dual_wind.wgsl:94-117), else the scan.
+//
+// The separated Hanna-record -> Langevin path (fpg_dispatch_hanna_params,
+// fpg_langevin_with_hanna) lives here too: it must give the fused kernel's
+// bits, so it is built with the same division (this unit's compile flags).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -30,6 +34,7 @@
 
 #include "fpg_internal.h"
 #include "physics.cuh"
+#include "slots.cuh"
 #include "step_core.cuh"
 
 namespace fpg {
@@ -550,6 +555,30 @@ struct RecordTurbArgs {
     uint32_t key0, key1;
 };
 
+// hanna_params.wgsl:231-258 with compute_hanna (physics/hanna.rs:49-163):
+// one 64-byte HannaParams record per slot, zeros for inactive slots.
+__global__ void __launch_bounds__(256) hanna_params_kernel(SlotView v, const float4* __restrict__ pbl, uint32_t pnx,
+                                                           uint32_t pny, fpg_hanna_params* __restrict__ out) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= v.n) return;
+    float4* o = reinterpret_cast<float4*>(out + p);
+    if ((v.flags[p] & FLAG_ACTIVE) == 0u) {
+        const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        o[0] = z; o[1] = z; o[2] = z; o[3] = z;
+        return;
+    }
+    const float4 cell = pbl_cell(v, p, pbl, pnx, pny);
+    const float ol = obukhov_from_inverse(cell.w);
+    const float z = v.pos_z[p];
+    const Hanna hn = compute_hanna(cell.x, cell.y, ol, cell.z, z);
+    // zeta and d(sigma_w^2)/dz as the CPU routine forms them (hanna.rs:55,145)
+    const float zeta = clampf(clampf(z, 0.0f, hn.h) / hn.h, 0.0f, 1.0f);
+    o[0] = make_float4(hn.ust, hn.wst, hn.ol, hn.h);
+    o[1] = make_float4(zeta, hn.sigu, hn.sigv, hn.sigw);
+    o[2] = make_float4(hn.dsigwdz, 2.0f * hn.sigw * hn.dsigwdz, hn.tlu, hn.tlv);
+    o[3] = make_float4(hn.tlw, 0.0f, 0.0f, 0.0f);
+}
+
 // langevin.wgsl:307-424: the turbulence update from a HannaParams record per
 // slot (the separated Hanna -> Langevin path of the reference's validation
 // and backward loops), with the fused kernel's Philox block layout and
@@ -621,6 +650,24 @@ extern "C" fpg_status fpg_langevin_with_hanna(fpg_ctx* ctx, fpg_particles* P, co
     ctx->count();
     FPG_CHECK_LAUNCH();
     if (next_counter) counter_add64(base_counter, (uint64_t)n * (n_substeps <= 2u ? 1u : 2u), next_counter);
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_dispatch_hanna_params(fpg_ctx* ctx, const fpg_particles* P, const fpg_pbl* pbl,
+                                                fpg_hanna_params* out_dev, size_t n_out, void* stream) {
+    if (!ctx || !P || !pbl) return FPG_ERR_INVALID_ARGUMENT;
+    if (P->dispatch == 0) return FPG_OK;
+    if (n_out != P->dispatch) return FPG_ERR_LENGTH_MISMATCH;
+    if (!out_dev || !aligned16(out_dev)) return FPG_ERR_INVALID_ARGUMENT;
+    if (pbl->nx == 0 || pbl->ny == 0) return FPG_ERR_ZERO_SHAPE;
+    if (pbl->nx > UINT32_MAX || pbl->ny > UINT32_MAX || P->dispatch > UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
+    if (!pbl->ready) return FPG_ERR_NOT_READY;
+    const SlotView v = slot_view(P);
+    if (v.n == 0) return FPG_OK;
+    hanna_params_kernel<<<(unsigned)((v.n + 255) / 256), 256, 0, ctx->pick(stream)>>>(
+        v, pbl->packed, (uint32_t)pbl->nx, (uint32_t)pbl->ny, out_dev);
+    ctx->count();
+    FPG_CHECK_LAUNCH();
     return FPG_OK;
 }
 
