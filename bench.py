@@ -58,13 +58,13 @@ BYTES_PER_PARTICLE_STEP = 96  # read 44 B + write 52 B of SoA state, one species
 ADJOINT_HBM_BUDGET = 140e9  # device bytes the batched adjoint may hold (the 150 GB budget, with margin)
 SORT_EVERY = 12  # steps between spatial reorders (divides the default 24 timed steps after 4 warm-up)
 # DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
-# an ncu capture of a 2 M-particle launch (135.1 MB), scaled by the particle
+# an ncu capture of a 2 M-particle launch (130.5 MB), scaled by the particle
 # count; below the algorithmic 96 B because part of the state was still in
 # the 126 MB L2 across the capture's replay passes.
-DRAM_BYTES_PER_PARTICLE_NCU = 135.1e6 / 2.0e6
+DRAM_BYTES_PER_PARTICLE_NCU = 130.5e6 / 2.0e6
 # Warp instructions per 32 particle-steps of fused_step_kernel
-# (smsp__inst_executed.sum of the same capture: 176.8 M for 2 M particles).
-WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 176.8e6 / (2.0e6 / 32)
+# (smsp__inst_executed.sum of the same capture: 171.4 M for 2 M particles).
+WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 171.4e6 / (2.0e6 / 32)
 
 
 def issue_roofline(n_particles, kernel_ms, clk):
