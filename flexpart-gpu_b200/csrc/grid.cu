@@ -40,9 +40,31 @@ __device__ __forceinline__ uint32_t cell_of(const GridArgs& a, const float* h, u
 constexpr uint32_t kSlotsPerThread = 2;
 
 // Each CTA bins one contiguous chunk of slots, two slots per thread per
-// pass with every field loaded up front (four per pass measured no
-// faster).  All sums are u32, so the grid does not depend on the order of
+// pass.  The fields of the next pass are loaded before the current pass's
+// run sums and table updates, so a thread always has a pass of loads in
+// flight.  All sums are u32, so the grid does not depend on the order of
 // the additions.
+struct SlotFields {
+    uint32_t f[kSlotsPerThread];
+    int32_t cx[kSlotsPerThread], cy[kSlotsPerThread];
+    float z[kSlotsPerThread], m[kSlotsPerThread];
+};
+
+__device__ __forceinline__ void load_pass(const GridArgs& a, uint64_t base, uint64_t end, SlotFields& s) {
+#pragma unroll
+    for (int j = 0; j < (int)kSlotsPerThread; ++j) {
+        const uint64_t p = base + (uint64_t)j * blockDim.x + threadIdx.x;
+        s.f[j] = 0u;
+        if (p < end) {
+            s.f[j] = a.flags[p];
+            s.cx[j] = a.cell_x[p];
+            s.cy[j] = a.cell_y[p];
+            s.z[j] = a.pos_z[p];
+            s.m[j] = a.mass[p];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, uint32_t chunk,
                                                    uint32_t* __restrict__ counts, uint32_t* __restrict__ mass) {
     __shared__ float s_h[FPG_MAX_LEVELS];
@@ -53,29 +75,27 @@ __global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, ui
         t_cnt[i] = 0u;
         t_mass[i] = 0u;
     }
-    __syncthreads();
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t begin = (uint64_t)blockIdx.x * chunk;
     const uint64_t end = min(begin + chunk, (uint64_t)a.n);
-    for (uint64_t base = begin; base < end; base += kSlotsPerThread * blockDim.x) {  // uniform across the CTA
+    const uint64_t pass = (uint64_t)kSlotsPerThread * blockDim.x;
+    SlotFields cur;
+    load_pass(a, begin, end, cur);
+    __syncthreads();
+    for (uint64_t base = begin; base < end; base += pass) {      // uniform across the CTA
         uint32_t key[kSlotsPerThread], q[kSlotsPerThread];
 #pragma unroll
         for (int j = 0; j < (int)kSlotsPerThread; ++j) {
-            const uint64_t p = base + (uint64_t)j * blockDim.x + threadIdx.x;
             key[j] = kEmpty;
             q[j] = 0u;
-            if (p < end) {
-                const uint32_t f = a.flags[p];
-                const int32_t cx = a.cell_x[p], cy = a.cell_y[p];
-                const float z = a.pos_z[p], m = a.mass[p];
-                if (f & 1u) {
-                    const uint32_t ix = (uint32_t)min(max(cx, 0), (int)a.nx - 1);
-                    const uint32_t iy = (uint32_t)min(max(cy, 0), (int)a.ny - 1);
-                    key[j] = (ix * a.ny + iy) * a.nz + level_of(z, s_h, a.nz, a.meters);
-                    q[j] = quantize(fmaxf(m, 0.0f), a.mass_scale);
-                }
+            if (cur.f[j] & 1u) {
+                const uint32_t ix = (uint32_t)min(max(cur.cx[j], 0), (int)a.nx - 1);
+                const uint32_t iy = (uint32_t)min(max(cur.cy[j], 0), (int)a.ny - 1);
+                key[j] = (ix * a.ny + iy) * a.nz + level_of(cur.z[j], s_h, a.nz, a.meters);
+                q[j] = quantize(fmaxf(cur.m[j], 0.0f), a.mass_scale);
             }
         }
+        if (base + pass < end) load_pass(a, base + pass, end, cur);
 #pragma unroll
         for (int j = 0; j < (int)kSlotsPerThread; ++j) warp_runs_add(key[j], q[j], lane, t_key, t_cnt, t_mass, counts, mass);
     }
