@@ -73,7 +73,7 @@ __device__ __forceinline__ D2 xcbrt(const D2& x) {
     return D2(c, x.a == 0.0f ? 0.0f : x.a * k, x.b == 0.0f ? 0.0f : x.b * k);
 }
 __device__ __forceinline__ D2 xpow(const D2& x, float e) {
-    const float p = powf(x.v, e);
+    const float p = pow_pos(x.v, e);
     const float k = __fdividef(e * p, x.v);
     return D2(p, x.a == 0.0f ? 0.0f : x.a * k, x.b == 0.0f ? 0.0f : x.b * k);
 }

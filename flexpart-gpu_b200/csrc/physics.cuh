@@ -6,8 +6,10 @@
 // as written, and the only fused operation is the explicit fmaf of lerp()
 // (the reference CPU lerp is `a.mul_add(1 - t, b * t)`,
 // src/physics/interpolation.rs:75-77, src/io/temporal.rs:417-420).
-// Transcendentals are CUDA's accurate expf/logf/powf/sincosf/cbrtf (no
-// fast-math intrinsics); sqrtf and '/' are correctly rounded.
+// Transcendentals are CUDA's accurate expf/logf/exp2f/log2f/sincosf/cbrtf
+// (no fast-math intrinsics); sqrtf is correctly rounded, and '/' is too
+// except in the step's units (step.cu, batch.cu, adjoint.cu), which the
+// build compiles with the approximate full-range division (within 2 ulp).
 #pragma once
 
 #include <cstdint>
@@ -84,7 +86,13 @@ __device__ __forceinline__ float val(float x) { return x; }
 __device__ __forceinline__ float xexp(float x) { return expf(x); }
 __device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ float xcbrt(float x) { return pow_third(x); }
-__device__ __forceinline__ float xpow(float x, float e) { return powf(x, e); }
+// x^e for x > 0 as 2^(e log2 x) from CUDA's exp2f and log2f: the reference's
+// pow(zeta, 0.8) of the stable-branch T_L (hanna.rs:111,
+// langevin_fused.wgsl:271,332) within a few ulp of powf, at a
+// fraction of its cost (the stable branch runs up to four times per
+// particle-step).  x <= 0 goes to powf (0^0.8 = 0).
+__device__ __forceinline__ float pow_pos(float x, float e) { return x > 0.0f ? exp2f(e * log2f(x)) : powf(x, e); }
+__device__ __forceinline__ float xpow(float x, float e) { return pow_pos(x, e); }
 __device__ __forceinline__ float xmax(float x, float c) { return fmaxf(x, c); }
 __device__ __forceinline__ float xclamp(float x, float lo, float hi) { return clampf(x, lo, hi); }
 __device__ __forceinline__ float xabs(float x) { return fabsf(x); }
