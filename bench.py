@@ -61,13 +61,13 @@ ADJOINT_HBM_BUDGET = 140e9  # device bytes the batched adjoint may hold (the 150
 # kernel slows by 2 % as the order decays, the reorder costs 0.92 ms)
 SORT_EVERY = 24
 # DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
-# an ncu capture of a 2 M-particle launch (130.5 MB), scaled by the particle
+# an ncu capture of a 2 M-particle launch (131.1 MB), scaled by the particle
 # count; below the algorithmic 96 B because part of the state was still in
 # the 126 MB L2 across the capture's replay passes.
-DRAM_BYTES_PER_PARTICLE_NCU = 130.5e6 / 2.0e6
+DRAM_BYTES_PER_PARTICLE_NCU = 131.1e6 / 2.0e6
 # Warp instructions per 32 particle-steps of fused_step_kernel
-# (smsp__inst_executed.sum of the same capture: 171.4 M for 2 M particles).
-WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 171.4e6 / (2.0e6 / 32)
+# (smsp__inst_executed.sum of the same capture: 158.3 M for 2 M particles).
+WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 158.3e6 / (2.0e6 / 32)
 
 
 def issue_roofline(n_particles, kernel_ms, clk):
