@@ -542,6 +542,11 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
         std::memcpy(report->next_philox_counter, d->counter, sizeof(d->counter));
     }
     mark(d, 6);
+    // the step is done: advance the clock before the timing read-back, so a
+    // failed read leaves the driver consistent
+    const uint64_t step_index = d->step_index;
+    d->step_index += 1;
+    d->t += d->direction > 0 ? d->cfg.timestep_seconds : -d->cfg.timestep_seconds;
     if (d->profile) {
         // StepTimingReport (timeloop.rs:398-467): device sections from the events
         const double host_ms =
@@ -556,7 +561,7 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
         float total = 0.0f;
         FPG_CUDA(cudaEventElapsedTime(&total, d->marks[0], d->marks[6]));
         fpg_step_timing& t = d->last_timing;
-        t.step_index = d->step_index;
+        t.step_index = step_index;
         t.sort_ms = sec[0]; t.release_ms = sec[1]; t.met_bracket_ms = sec[2];
         t.pbl_ms = sec[3]; t.step_ms = sec[4]; t.compaction_ms = sec[5];
         t.gpu_total_ms = total;
@@ -570,8 +575,6 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
                          (unsigned long long)t.step_index, t.sort_ms, t.release_ms, t.met_bracket_ms, t.pbl_ms,
                          t.step_ms, t.compaction_ms, t.gpu_total_ms, t.host_call_ms, t.wall_ms);
     }
-    d->step_index += 1;
-    d->t += d->direction > 0 ? d->cfg.timestep_seconds : -d->cfg.timestep_seconds;
     return FPG_OK;
 }
 
