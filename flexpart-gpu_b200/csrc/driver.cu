@@ -117,6 +117,10 @@ struct fpg_forward {
     bool profile = false, print_profile = false, have_timing = false;
     cudaEvent_t marks[7] = {};
     fpg_step_timing last_timing{};
+    // validation mode (fpg_forward_set_validation_mode / FLEXPART_GPU_VALIDATION=1):
+    // separated passes with a per-slot Hanna record buffer (capacity records)
+    bool validation = false;
+    fpg_hanna_params* hanna_records = nullptr;
 };
 
 namespace {
@@ -205,6 +209,7 @@ extern "C" fpg_status fpg_forward_destroy(fpg_forward* d) {
     }
     for (cudaEvent_t e : d->marks)
         if (e) cudaEventDestroy(e);
+    cudaFree(d->hanna_records);
     delete d;
     return FPG_OK;
 }
@@ -216,6 +221,14 @@ extern "C" fpg_status fpg_forward_set_profiling(fpg_forward* d, int32_t on) {
         if (st != FPG_OK) return st;
     }
     d->profile = on != 0;
+    return FPG_OK;
+}
+
+extern "C" fpg_status fpg_forward_set_validation_mode(fpg_forward* d, int32_t on) {
+    if (!d) return FPG_ERR_INVALID_ARGUMENT;
+    if (on && !d->hanna_records)
+        FPG_CUDA(cudaMalloc(&d->hanna_records, (d->capacity > 0 ? d->capacity : 1) * sizeof(fpg_hanna_params)));
+    d->validation = on != 0;
     return FPG_OK;
 }
 
@@ -276,6 +289,9 @@ static fpg_status driver_create(fpg_ctx* ctx, const fpg_forward_config* cfg, con
         st = fpg_forward_set_profiling(d, 1);
         d->print_profile = true;
     }
+    // is_validation_mode (timeloop.rs:480-494)
+    const char* val = std::getenv("FLEXPART_GPU_VALIDATION");
+    if (st == FPG_OK && val && std::strcmp(val, "1") == 0) st = fpg_forward_set_validation_mode(d, 1);
     if (st != FPG_OK) {
         fpg_forward_destroy(d);
         return st;
@@ -497,7 +513,26 @@ extern "C" fpg_status fpg_forward_run_timestep(fpg_forward* d, const fpg_met_bra
     const size_t ref_dispatch = d->compaction ? d->active : d->capacity;
     d->particles->dispatch = d->next_free;
     uint32_t ignored[4];
-    st = fpg_step(d->ctx, d->particles, d->met, d->pbl, &p, ignored, nullptr);
+    if (d->validation) {
+        // the validation path (timeloop.rs:1128-1155): advection, Hanna
+        // records, the Langevin update from the records, deposition, each a
+        // pass of its own; the same bits as the fused kernel
+        fpg_step_params pa = p;
+        pa.stages = FPG_STAGE_ADVECT;
+        st = fpg_step(d->ctx, d->particles, d->met, nullptr, &pa, nullptr, nullptr);
+        const size_t n = d->particles->dispatch;
+        if (st == FPG_OK)
+            st = fpg_dispatch_hanna_params(d->ctx, d->particles, d->pbl, d->hanna_records, n, nullptr);
+        if (st == FPG_OK)
+            st = fpg_langevin_with_hanna(d->ctx, d->particles, d->hanna_records, n, p.turb_dt_seconds,
+                                         p.rho_grad_over_rho, p.n_substeps, p.min_height_m, p.key, p.counter,
+                                         ignored, nullptr);
+        fpg_step_params pd = p;
+        pd.stages = FPG_STAGE_DRY | FPG_STAGE_WET;
+        if (st == FPG_OK) st = fpg_step(d->ctx, d->particles, nullptr, nullptr, &pd, nullptr, nullptr);
+    } else {
+        st = fpg_step(d->ctx, d->particles, d->met, d->pbl, &p, ignored, nullptr);
+    }
     d->particles->dispatch = ref_dispatch;
     if (st != FPG_OK) return st;
     if (ref_dispatch > 0) {

@@ -163,6 +163,7 @@ _sig("fpg_forward_met_ring", _i32, _vp, _u32)
 _sig("fpg_forward_prefetch_frame", _i32, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp)
 _sig("fpg_forward_met_ring_stats", _i32, _vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64))
 _sig("fpg_forward_set_profiling", _i32, _vp, _i32)
+_sig("fpg_forward_set_validation_mode", _i32, _vp, _i32)
 _sig("fpg_forward_last_timing", _i32, _vp, _vp)
 _sig("fpg_host_alloc", _i32, _vp, _sz, ctypes.POINTER(_vp))
 _sig("fpg_host_free", _i32, _vp, _vp)
@@ -209,7 +210,7 @@ EXPORTED_DRIVER = [
     "fpg_forward_current_time", "fpg_forward_run_timestep", "fpg_forward_finalize", "fpg_forward_particles",
     "fpg_forward_accumulate_grid", "fpg_parse_timestamp",
     "fpg_forward_met_ring", "fpg_forward_prefetch_frame", "fpg_forward_met_ring_stats",
-    "fpg_forward_set_profiling", "fpg_forward_last_timing",
+    "fpg_forward_set_profiling", "fpg_forward_last_timing", "fpg_forward_set_validation_mode",
     "fpg_backward_config_default", "fpg_backward_create", "fpg_backward_destroy", "fpg_backward_has_remaining_steps",
     "fpg_backward_current_time", "fpg_backward_run_timestep", "fpg_backward_particles",
     "fpg_batch_create", "fpg_batch_destroy", "fpg_batch_upload_frame", "fpg_batch_run", "fpg_batch_run_sequential",

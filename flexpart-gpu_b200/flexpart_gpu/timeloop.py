@@ -120,6 +120,12 @@ class ForwardDriver:
         its device work); also on when FLEXPART_GPU_PROFILE=1 at creation."""
         check(lib.fpg_forward_set_profiling(self.h, 1 if on else 0), "fpg_forward_set_profiling")
 
+    def set_validation_mode(self, on: bool = True):
+        """The reference's validation path: separated advection, Hanna-record,
+        Langevin and deposition passes (the fused kernel's bits); also on when
+        FLEXPART_GPU_VALIDATION=1 at creation."""
+        check(lib.fpg_forward_set_validation_mode(self.h, 1 if on else 0), "fpg_forward_set_validation_mode")
+
     def last_timing(self) -> StepTiming:
         """The timing of the last step run with profiling on."""
         t = StepTiming()

@@ -177,6 +177,14 @@ typedef struct fpg_step_timing {
  * With timing on, every run_timestep waits for its device work to finish.
  * NVTX ranges mark every step and section whether timing is on or not. */
 fpg_status fpg_forward_set_profiling(fpg_forward* d, int32_t on);
+/* The reference's validation mode (is_validation_mode, timeloop.rs:480-494,
+ * used at :1128-1155): each step runs advection, the per-slot Hanna records
+ * (fpg_dispatch_hanna_params), the Langevin update from those records
+ * (fpg_langevin_with_hanna) and deposition as separate passes instead of the
+ * fused kernel.  The results are the fused kernel's, bit for bit.  Also on
+ * when FLEXPART_GPU_VALIDATION=1 at create time.  Turning it on allocates
+ * one 64-byte Hanna record per slot of the capacity. */
+fpg_status fpg_forward_set_validation_mode(fpg_forward* d, int32_t on);
 /* The timing of the last run_timestep made with timing on; NOT_READY if none. */
 fpg_status fpg_forward_last_timing(const fpg_forward* d, fpg_step_timing* out);
 

@@ -268,3 +268,66 @@ def test_profile_environment_variable_prints_one_line_per_step(tmp_path):
     lines = [ln for ln in r.stderr.splitlines() if ln.startswith("[profile] step=")]
     assert steps > 0 and len(lines) == steps
     assert all("step=" in ln and "gpu=" in ln and "total=" in ln for ln in lines)
+
+
+@pytest.mark.parametrize("mode", ["plain", "compaction_sort"])
+def test_validation_mode_gives_the_fused_kernels_bits(ctx, mode):
+    """The reference's validation path (separated advection, Hanna records,
+    Langevin from the records, deposition; timeloop.rs:1128-1155) against the
+    fused kernel: identical reports and particle bytes after every step."""
+    scn = _small(particles=20_000, hours=4)
+    frames = synthetic.make_frames(scn.met)
+    kw = {"use_compaction": 1, "sort_interval_steps": 3} if mode == "compaction_sort" else {}
+    fused, sep = _driver(ctx, scn, **kw), _driver(ctx, scn, **kw)
+    sep.set_validation_mode(True)
+    src = tl.BracketSource(scn, frames)
+    forcing = tl.uniform_forcing(dry_velocity=0.002, wet_lambda=2e-4, wet_fraction=0.6)
+    steps = 0
+    while fused.has_remaining_steps:
+        ra = fused.run_timestep(src.at(fused.current_time_seconds), forcing)
+        rb = sep.run_timestep(src.at(sep.current_time_seconds), forcing)
+        assert (ra.released_count, ra.active_particle_count, list(ra.next_philox_counter)) == \
+               (rb.released_count, rb.active_particle_count, list(rb.next_philox_counter))
+        assert fused.particles.download().tobytes() == sep.particles.download().tobytes(), steps
+        steps += 1
+    assert steps == 17 and not sep.has_remaining_steps
+
+
+def test_validation_environment_variable_selects_the_separated_path(tmp_path):
+    """FLEXPART_GPU_VALIDATION=1 at creation (is_validation_mode,
+    timeloop.rs:480-494) runs the separated path; its particles equal the
+    fused run's."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = tmp_path / "run.py"
+    script.write_text(
+        "import sys\nimport numpy as np\n"
+        "from flexpart_gpu import api, synthetic, timeloop as tl\n"
+        "scn = synthetic.config0()\n"
+        "scn.sources[0].particle_count = 5000\nscn.capacity = 5000\nscn.end = scn.start + 2 * 3600\n"
+        "frames = synthetic.make_frames(scn.met)\n"
+        "ctx = api.Context(0)\n"
+        "drv = tl.ForwardDriver(ctx, tl.scenario_config(scn), tl.scenario_releases(scn), tl.scenario_domain(scn),\n"
+        "                       scn.capacity, (scn.met.nx, scn.met.ny, scn.met.nz),\n"
+        "                       synthetic.level_heights(scn.met.nz, scn.met.top_m))\n"
+        "src = tl.BracketSource(scn, frames)\n"
+        "while drv.has_remaining_steps:\n"
+        "    drv.run_timestep(src.at(drv.current_time_seconds), tl.uniform_forcing(dry_velocity=0.002))\n"
+        "np.save(sys.argv[1], drv.particles.download())\n"
+        "print('launches', ctx.kernel_launches)\n")
+    runs, launches = {}, {}
+    for label, flag in (("separated", "1"), ("fused", "0")):
+        env = dict(os.environ, FLEXPART_GPU_VALIDATION=flag,
+                   PYTHONPATH=os.pathsep.join([root, os.path.join(root, "flexpart-gpu_b200")]))
+        path = tmp_path / f"{label}.npy"
+        r = subprocess.run([sys.executable, str(script), str(path)], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        runs[label] = np.load(path)
+        launches[label] = int(r.stdout.split()[-1])
+    assert runs["separated"].tobytes() == runs["fused"].tobytes()
+    assert launches["separated"] > launches["fused"]       # three more passes per step
+    assert (runs["fused"]["flags"] & 1).sum() == 5000
