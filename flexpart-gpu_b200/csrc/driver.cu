@@ -281,7 +281,11 @@ static fpg_status driver_create(fpg_ctx* ctx, const fpg_forward_config* cfg, con
     if (st == FPG_OK && heights) st = fpg_met_set_level_heights(d->met, heights, nz);
     if (st == FPG_OK) st = fpg_surface_create(ctx, nx, ny, &d->surface);
     if (st == FPG_OK) st = fpg_pbl_create(ctx, nx, ny, &d->pbl);
-    if (st == FPG_OK && cfg->use_compaction) st = fpg_compaction_create(ctx, capacity, &d->compaction);
+    // is_compaction_enabled (timeloop.rs:496-513): FLEXPART_GPU_COMPACTION=1 turns
+    // compaction on as the configuration's use_compaction does
+    const char* cmp = std::getenv("FLEXPART_GPU_COMPACTION");
+    const bool compaction = cfg->use_compaction || (cmp && std::strcmp(cmp, "1") == 0);
+    if (st == FPG_OK && compaction) st = fpg_compaction_create(ctx, capacity, &d->compaction);
     if (st == FPG_OK && cfg->sort_interval_steps) st = fpg_sorter_create(ctx, capacity, &d->sorter);
     // is_profiling_enabled (timeloop.rs:469-476)
     const char* prof = std::getenv("FLEXPART_GPU_PROFILE");

@@ -53,7 +53,8 @@ typedef struct fpg_forward_config {
     uint32_t philox_key[2];
     uint32_t initial_philox_counter[4];
     uint32_t sort_interval_steps;         /* 0: no spatial reorder */
-    int32_t use_compaction;               /* FLEXPART_GPU_COMPACTION (timeloop.rs:506-513) */
+    int32_t use_compaction;               /* is_compaction_enabled (timeloop.rs:506-513); FLEXPART_GPU_COMPACTION=1
+                                             at create turns it on as well */
     uint32_t n_substeps;                  /* 4 in production (timeloop.rs:1111) */
     float min_height_m;                   /* 0.01 in production (timeloop.rs:1112) */
 } fpg_forward_config;

@@ -293,10 +293,10 @@ def test_validation_mode_gives_the_fused_kernels_bits(ctx, mode):
     assert steps == 17 and not sep.has_remaining_steps
 
 
-def test_validation_environment_variable_selects_the_separated_path(tmp_path):
+def test_environment_variables_select_the_separated_path_and_compaction(tmp_path):
     """FLEXPART_GPU_VALIDATION=1 at creation (is_validation_mode,
-    timeloop.rs:480-494) runs the separated path; its particles equal the
-    fused run's."""
+    timeloop.rs:480-494) runs the separated path, FLEXPART_GPU_COMPACTION=1
+    the compaction (as the configuration's use_compaction does)."""
     import os
     import subprocess
     import sys
@@ -310,8 +310,9 @@ def test_validation_environment_variable_selects_the_separated_path(tmp_path):
         "scn.sources[0].particle_count = 5000\nscn.capacity = 5000\nscn.end = scn.start + 2 * 3600\n"
         "frames = synthetic.make_frames(scn.met)\n"
         "ctx = api.Context(0)\n"
-        "drv = tl.ForwardDriver(ctx, tl.scenario_config(scn), tl.scenario_releases(scn), tl.scenario_domain(scn),\n"
-        "                       scn.capacity, (scn.met.nx, scn.met.ny, scn.met.nz),\n"
+        "kw = {'use_compaction': 1} if sys.argv[2] == 'cfg_compaction' else {}\n"
+        "drv = tl.ForwardDriver(ctx, tl.scenario_config(scn, **kw), tl.scenario_releases(scn),\n"
+        "                       tl.scenario_domain(scn), scn.capacity, (scn.met.nx, scn.met.ny, scn.met.nz),\n"
         "                       synthetic.level_heights(scn.met.nz, scn.met.top_m))\n"
         "src = tl.BracketSource(scn, frames)\n"
         "while drv.has_remaining_steps:\n"
@@ -319,15 +320,23 @@ def test_validation_environment_variable_selects_the_separated_path(tmp_path):
         "np.save(sys.argv[1], drv.particles.download())\n"
         "print('launches', ctx.kernel_launches)\n")
     runs, launches = {}, {}
-    for label, flag in (("separated", "1"), ("fused", "0")):
-        env = dict(os.environ, FLEXPART_GPU_VALIDATION=flag,
-                   PYTHONPATH=os.pathsep.join([root, os.path.join(root, "flexpart-gpu_b200")]))
+    for label, flags in (("separated", {"FLEXPART_GPU_VALIDATION": "1"}), ("fused", {}),
+                         ("compaction_env", {"FLEXPART_GPU_COMPACTION": "1"}), ("cfg_compaction", {})):
+        env = dict(os.environ, PYTHONPATH=os.pathsep.join([root, os.path.join(root, "flexpart-gpu_b200")]))
+        env.pop("FLEXPART_GPU_VALIDATION", None)
+        env.pop("FLEXPART_GPU_COMPACTION", None)
+        env.update(flags)
         path = tmp_path / f"{label}.npy"
-        r = subprocess.run([sys.executable, str(script), str(path)], env=env, capture_output=True, text=True,
-                           timeout=300)
+        r = subprocess.run([sys.executable, str(script), str(path), label], env=env, capture_output=True,
+                           text=True, timeout=300)
         assert r.returncode == 0, r.stderr[-2000:]
         runs[label] = np.load(path)
         launches[label] = int(r.stdout.split()[-1])
     assert runs["separated"].tobytes() == runs["fused"].tobytes()
     assert launches["separated"] > launches["fused"]       # three more passes per step
+    # FLEXPART_GPU_COMPACTION=1 (is_compaction_enabled, timeloop.rs:496-513) is
+    # the configuration's use_compaction: the same compacted run (its Philox
+    # counter advances by the active count, not the capacity)
+    assert runs["compaction_env"].tobytes() == runs["cfg_compaction"].tobytes()
+    assert launches["compaction_env"] == launches["cfg_compaction"] > launches["fused"]
     assert (runs["fused"]["flags"] & 1).sum() == 5000
