@@ -95,6 +95,15 @@ class ForwardDriver:
     def finalize(self):
         check(lib.fpg_forward_finalize(self.h), "fpg_forward_finalize")
 
+    def run_to_end(self, met: MetBracket, forcing: Forcing) -> list[StepReport]:
+        """run_to_end (timeloop.rs:1318-1333): every remaining step with one met
+        bracket and forcing, then finalize; the steps' reports."""
+        reports = []
+        while self.has_remaining_steps:
+            reports.append(self.run_timestep(met, forcing))
+        self.finalize()
+        return reports
+
     def enable_met_ring(self, n_slots: int = 3):
         """Met streaming: a device ring of n_slots frames filled ahead of use."""
         check(lib.fpg_forward_met_ring(self.h, n_slots), "fpg_forward_met_ring")
@@ -187,6 +196,14 @@ class BackwardDriver:
                                             col), "fpg_backward_run_timestep")
         return rep, [(int(c.hit_count), float(c.total_mass_kg), float(c.total_mass_kg_f64))
                      for c in col[: self.n_regions]]
+
+    def run_to_end(self, met: MetBracket, forcing: Forcing):
+        """run_to_end (timeloop.rs:1828-1838): every remaining step with one met
+        bracket and forcing; the steps' (report, collections) pairs."""
+        out = []
+        while self.has_remaining_steps:
+            out.append(self.run_timestep(met, forcing))
+        return out
 
 
 def backward_config(**kw) -> BackwardConfig:

@@ -340,3 +340,25 @@ def test_environment_variables_select_the_separated_path_and_compaction(tmp_path
     assert runs["compaction_env"].tobytes() == runs["cfg_compaction"].tobytes()
     assert launches["compaction_env"] == launches["cfg_compaction"] > launches["fused"]
     assert (runs["fused"]["flags"] & 1).sum() == 5000
+
+
+def test_run_to_end_with_one_bracket_equals_the_manual_loop(ctx):
+    """run_to_end (timeloop.rs:1318-1333): one met bracket and forcing for
+    every remaining step (times past the bracket clamped), then finalize; the
+    same reports and particles as stepping by hand."""
+    scn = _small(particles=10_000, hours=2)
+    frames = synthetic.make_frames(scn.met)
+    src = tl.BracketSource(scn, frames)
+    met = src.at(scn.start)
+    forcing = tl.uniform_forcing(dry_velocity=0.002)
+    a, b = _driver(ctx, scn, clamp_time_bounds=1), _driver(ctx, scn, clamp_time_bounds=1)
+    reports = a.run_to_end(met, forcing)
+    manual = []
+    while b.has_remaining_steps:
+        manual.append(b.run_timestep(met, forcing))
+    b.finalize()
+    assert len(reports) == len(manual) == 9 and not a.has_remaining_steps
+    for ra, rb in zip(reports, manual):
+        assert (ra.step_index, ra.released_count, ra.interpolation_alpha, list(ra.next_philox_counter)) == \
+               (rb.step_index, rb.released_count, rb.interpolation_alpha, list(rb.next_philox_counter))
+    assert a.particles.download().tobytes() == b.particles.download().tobytes()
