@@ -853,6 +853,10 @@ extern "C" int32_t fpg_backward_has_remaining_steps(const fpg_backward* b) {
 extern "C" int64_t fpg_backward_current_time(const fpg_backward* b) { return b ? fpg_forward_current_time(b->f) : 0; }
 extern "C" fpg_particles* fpg_backward_particles(fpg_backward* b) { return b ? b->f->particles : nullptr; }
 
+extern "C" fpg_status fpg_backward_set_validation_mode(fpg_backward* b, int32_t on) {
+    return b ? fpg_forward_set_validation_mode(b->f, on) : FPG_ERR_INVALID_ARGUMENT;
+}
+
 extern "C" fpg_status fpg_backward_run_timestep(fpg_backward* b, const fpg_met_bracket* met, const fpg_forcing* f,
                                                 fpg_step_report* report, fpg_source_collection* out) {
     if (!b) return FPG_ERR_INVALID_ARGUMENT;

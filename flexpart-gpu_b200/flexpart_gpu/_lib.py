@@ -159,6 +159,7 @@ _sig("fpg_backward_has_remaining_steps", _i32, _vp)
 _sig("fpg_backward_current_time", ctypes.c_int64, _vp)
 _sig("fpg_backward_run_timestep", _i32, _vp, _vp, _vp, _vp, _vp)
 _sig("fpg_backward_particles", _vp, _vp)
+_sig("fpg_backward_set_validation_mode", _i32, _vp, _i32)
 _sig("fpg_forward_met_ring", _i32, _vp, _u32)
 _sig("fpg_forward_prefetch_frame", _i32, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp)
 _sig("fpg_forward_met_ring_stats", _i32, _vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64))
@@ -213,6 +214,7 @@ EXPORTED_DRIVER = [
     "fpg_forward_set_profiling", "fpg_forward_last_timing", "fpg_forward_set_validation_mode",
     "fpg_backward_config_default", "fpg_backward_create", "fpg_backward_destroy", "fpg_backward_has_remaining_steps",
     "fpg_backward_current_time", "fpg_backward_run_timestep", "fpg_backward_particles",
+    "fpg_backward_set_validation_mode",
     "fpg_batch_create", "fpg_batch_destroy", "fpg_batch_upload_frame", "fpg_batch_run", "fpg_batch_run_sequential",
     "fpg_batch_steps_done", "fpg_batch_scenario_slots", "fpg_batch_particles", "fpg_batch_download_grids",
     "fpg_batch_errors", "fpg_batch_tuning_candidates", "fpg_batch_autotune", "fpg_batch_set_tuning",

@@ -197,6 +197,11 @@ class BackwardDriver:
         return rep, [(int(c.hit_count), float(c.total_mass_kg), float(c.total_mass_kg_f64))
                      for c in col[: self.n_regions]]
 
+    def set_validation_mode(self, on: bool = True):
+        """The separated passes the reference's backward driver always runs
+        (timeloop.rs:1433-1437); the fused kernel's bits."""
+        check(lib.fpg_backward_set_validation_mode(self.h, 1 if on else 0), "fpg_backward_set_validation_mode")
+
     def run_to_end(self, met: MetBracket, forcing: Forcing):
         """run_to_end (timeloop.rs:1828-1838): every remaining step with one met
         bracket and forcing; the steps' (report, collections) pairs."""

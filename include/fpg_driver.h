@@ -267,6 +267,10 @@ int64_t fpg_backward_current_time(const fpg_backward* d);
 fpg_status fpg_backward_run_timestep(fpg_backward* d, const fpg_met_bracket* met, const fpg_forcing* forcing,
                                      fpg_step_report* report, fpg_source_collection* collections);
 fpg_particles* fpg_backward_particles(fpg_backward* d);
+/* The separated passes of fpg_forward_set_validation_mode for the backward
+ * step, the path the reference's backward driver always takes
+ * (timeloop.rs:1433-1437); the same bits as the fused kernel. */
+fpg_status fpg_backward_set_validation_mode(fpg_backward* d, int32_t on);
 
 /* ------------------------------------------------------------------------
  * Batched ensemble: many independent release scenarios stepped together.

@@ -213,3 +213,29 @@ def test_backward_validation_errors(ctx):
     assert status(tl.backward_config(start_seconds=T0 + 2, end_seconds=T0),
                   g=[SourceRegion(7.1, 6.9, 4.9, 5.1, 0.0, 5.0)]) == -22
     assert status(tl.backward_config(start_seconds=T0 + 2, end_seconds=T0, timestep_seconds=0)) == -2
+
+
+def test_backward_separated_passes_give_the_fused_bits(ctx):
+    """The reference's backward driver always runs the separated Hanna,
+    Langevin and deposition passes (timeloop.rs:1433-1437); with them the
+    device's particles and source collections equal the fused kernel's, bit
+    for bit, after every step."""
+    scn, oscn, receptors, regions = _config0_backward(hours=3, per_receptor=2_000)
+    spec = scn.met
+    frames = synthetic.make_frames(spec)
+    src = tl.BracketSource(scn, frames)
+    xs, ys, zs = synthetic.velocity_scale(spec)
+    cfg = tl.backward_config(start_seconds=oscn.start, end_seconds=oscn.end, timestep_seconds=900,
+                             x_grid_per_meter=xs, y_grid_per_meter=ys, z_grid_per_meter=zs, philox_key=(42, 0))
+    drivers = [tl.BackwardDriver(ctx, cfg, receptors, regions, tl.scenario_domain(scn), oscn.capacity,
+                                 (spec.nx, spec.ny, spec.nz), synthetic.level_heights(spec.nz, spec.top_m))
+               for _ in range(2)]
+    drivers[1].set_validation_mode(True)
+    forcing = tl.uniform_forcing(dry_velocity=0.002)
+    steps = 0
+    while drivers[0].has_remaining_steps:
+        (ra, ca), (rb, cb) = (d.run_timestep(src.at(d.current_time_seconds), forcing) for d in drivers)
+        assert list(ra.next_philox_counter) == list(rb.next_philox_counter) and ca == cb
+        assert drivers[0].particles.download().tobytes() == drivers[1].particles.download().tobytes(), steps
+        steps += 1
+    assert steps == 13
