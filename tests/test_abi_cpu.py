@@ -40,6 +40,11 @@ def test_null_handles_are_rejected():
     assert lib.fpg_step(None, None, None, None, None, None, None) == -1
     assert lib.fpg_particles_upload(None, 0, 0, None, None) == -1
     assert lib.fpg_grid_download(None, None, None, None, None) == -1
+    # the driver's timing and validation switches
+    assert lib.fpg_forward_set_profiling(None, 1) == -1
+    assert lib.fpg_forward_last_timing(None, None) == -1
+    assert lib.fpg_forward_set_validation_mode(None, 1) == -1
+    assert lib.fpg_backward_set_validation_mode(None, 1) == -1
 
 
 def test_record_layouts_match_the_c_header(tmp_path):
