@@ -56,10 +56,13 @@ METRIC = "particle-steps/s"
 UNIT = "particle-steps/s"
 BYTES_PER_PARTICLE_STEP = 96  # read 44 B + write 52 B of SoA state, one species
 ADJOINT_HBM_BUDGET = 140e9  # device bytes the batched adjoint may hold (the 150 GB budget, with margin)
-# steps between spatial reorders of the population: measured at 10 M particles,
-# a reorder every 24 steps gives more particle-steps/s than every 12 (the
-# kernel slows by 2 % as the order decays, the reorder costs 0.92 ms)
-SORT_EVERY = 24
+# steps between spatial reorders of the population (one per simulated day at
+# dt 900 s): measured at 10 M particles over 96 steps, a reorder every
+# 12 / 24 / 48 / 96 steps gives 1.059 / 1.079 / 1.097 / 1.103e10
+# particle-steps/s (the kernel averages 0.836 / 0.857 / 0.861 / 0.865 ms as
+# the order decays; a reorder costs 0.92 ms).  The default window of timed
+# steps is one reorder period, and its first step reorders.
+SORT_EVERY = 96
 # DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
 # an ncu capture of a 2 M-particle launch (131.1 MB), scaled by the particle
 # count; below the algorithmic 96 B because part of the state was still in
@@ -90,7 +93,7 @@ def issue_roofline(n_particles, kernel_ms, clk):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--steps", type=int, default=SORT_EVERY)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=10_000_000)
