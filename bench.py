@@ -109,6 +109,9 @@ def parse():
     ap.add_argument("--adjoint-instances", type=int, default=64)
     ap.add_argument("--quick", action="store_true",
                     help="profiling case: no spin-up (particles scattered around the sources), no e2e, no CPU leg")
+    ap.add_argument("--case", choices=["batched", "inverse"],
+                    help="small profiling case, then exit: batched = 64 scenarios (~3.5 M particles) for 48 steps; "
+                         "inverse = 200 k particles, 16 sources, 6 h, tape recorded in the forward")
     return ap.parse_args()
 
 
@@ -219,6 +222,152 @@ def oracle_steps(scn, frames, rec, threads, steps=None, seconds=None, counter0=0
     return times
 
 
+def legacy_steps(scn, frames, rec, threads, seconds):
+    """The reference's CPU pipeline as its benchmark runs it
+    (benches/advection.rs:1118-1213), restated over the oracle: the three
+    wind components time-interpolated over the whole grid
+    (interpolate_wind_field_linear), surface lerp + PBL diagnostics per cell,
+    advection on the interpolated wind, Hanna + legacy Langevin
+    (n_substeps = 0), dry and wet deposition from per-particle arrays, and
+    the CPU concentration grid.  Returns the seconds of each step."""
+    from flexpart_gpu import synthetic
+    from flexpart_gpu.records import StepParams
+    from oracle import orc
+
+    xs, ys, zs = synthetic.velocity_scale(scn.met)
+    st = orc.State.from_records(rec)
+    n = len(rec)
+    rng = np.random.default_rng(23)
+    dry_v = rng.uniform(0.001, 0.003, n).astype(np.float32)
+    wet_l = rng.uniform(0.0, 1e-3, n).astype(np.float32)
+    wet_f = (np.arange(n) % 100 / 100.0).astype(np.float32)
+    t = scn.end
+    times = []
+    t_start = time.perf_counter()
+    k = 0
+    while True:
+        fa, fb, met = oracle_met(scn, frames, t)
+        _, _, ta, tb = synthetic.bracket_frames(scn, t)
+        alpha = (t - ta) / float(tb - ta)
+        t0 = time.perf_counter()
+        wind = {c: orc.lerp_field(met[c + "0"], met[c + "1"], alpha, threads) for c in ("u", "v", "w")}
+        one = {"u0": wind["u"], "v0": wind["v"], "w0": wind["w"], "u1": wind["u"], "v1": wind["v"],
+               "w1": wind["w"], "heights": met["heights"]}
+        pbl = orc.pbl_diagnostics(frames[fa]["surface"], frames[fb]["surface"], alpha, scn.met.nx, scn.met.ny)
+        prm = StepParams.production(alpha=0.0, dt_seconds=float(scn.dt), turb_dt_seconds=float(scn.dt),
+                                    x_grid_per_meter=xs, y_grid_per_meter=ys, z_grid_per_meter=zs, key=scn.key,
+                                    counter=(2 * n * k, 0, 0, 0), n_substeps=0, dry_mode=2, wet_mode=2)
+        orc.step(st, n, one, pbl, prm, dry_velocity=dry_v, wet_lambda=wet_l, wet_fraction=wet_f, threads=threads)
+        orc.grid(st, n, 0, 1e6, scn.outheights, scn.out_shape)
+        times.append(time.perf_counter() - t0)
+        k += 1
+        t += scn.dt
+        el = time.perf_counter() - t_start
+        if el >= seconds or (k >= 3 and el * (k + 1) / k > 3 * seconds):
+            break
+    return times
+
+
+def host_cpu():
+    """CPU model name (lscpu, else /proc/cpuinfo) and whether a Rust toolchain
+    is present on this host."""
+    import shutil
+
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                model = line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    if model is None:
+        try:
+            for line in open("/proc/cpuinfo"):
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+        except Exception:
+            pass
+    return {"model": model, "logical_cpus": os.cpu_count(), "cargo": shutil.which("cargo")}
+
+
+def cpu_figures(scn, frames, rec, threads, seconds=5.0):
+    """Companion CPU numbers beside the main one: the production step on one
+    core, and the reference's legacy CPU pipeline on one core and on all."""
+    one = rec[:min(len(rec), 50_000)]
+    t1 = oracle_steps(scn, frames, one, 1, seconds=seconds)
+    out = {"production_1_core": {"value": len(one) * len(t1) / sum(t1), "unit": UNIT, "cores": 1,
+                                 "sample": f"{len(one)} particles x {len(t1)} steps"}}
+    for cores, sample in ((threads, rec), (1, one)):
+        tl_ = legacy_steps(scn, frames, sample, cores, seconds)
+        out[f"legacy_pipeline_{'1_core' if cores == 1 else 'all_cores'}"] = {
+            "value": len(sample) * len(tl_) / sum(tl_), "unit": UNIT, "cores": cores,
+            "sample": f"{len(sample)} particles x {len(tl_)} steps",
+            "pipeline": "whole-grid wind lerp, PBL per cell, advection, Hanna + legacy Langevin (no sub-steps), "
+                        "dry + wet from per-particle arrays, CPU grid (benches/advection.rs:1118-1213)"}
+    out["host"] = host_cpu()
+    return out
+
+
+def parity_sample(ctx, scn, frames, rec, t, counter):
+    """One production step of the sampled particles on the device and in the
+    oracle (FP32): the largest error per field, scaled as the parity tests
+    scale it (1 cell for grid positions, max(|z|, 100 m) for heights, 2 m/s
+    for velocities, the mass itself)."""
+    from flexpart_gpu import api, synthetic
+    from flexpart_gpu.records import StepParams
+    from oracle import orc
+
+    spec = scn.met
+    n = len(rec)
+    fa, fb, met = oracle_met(scn, frames, t)
+    _, _, ta, tb = synthetic.bracket_frames(scn, t)
+    alpha = (t - ta) / float(tb - ta)
+    xs, ys, zs = synthetic.velocity_scale(spec)
+    prm = StepParams.production(alpha=alpha, dt_seconds=float(scn.dt), turb_dt_seconds=float(scn.dt),
+                                x_grid_per_meter=xs, y_grid_per_meter=ys, z_grid_per_meter=zs, key=scn.key,
+                                counter=counter, dry_mode=1, dry_velocity_m_s=scn.dry_velocity, wet_mode=3)
+    precip = synthetic.precipitation(spec, fa)
+    m = api.Met(ctx, spec.nx, spec.ny, spec.nz)
+    m.set_level_heights(met["heights"])
+    m.upload_frame(0, met["u0"], met["v0"], met["w0"])
+    m.upload_frame(1, met["u1"], met["v1"], met["w1"])
+    surf = api.Surface(ctx, spec.nx, spec.ny)
+    surf.upload(0, frames[fa]["surface"])
+    surf.upload(1, frames[fb]["surface"])
+    pbl = api.Pbl(ctx, spec.nx, spec.ny)
+    api.pbl_diagnostics(ctx, surf, alpha, pbl)
+    wet = api.CellField(ctx, spec.nx, spec.ny)
+    wet.from_precipitation(precip, None, None, scn.wet_a, scn.wet_b)
+    parts = api.Particles(ctx, n)
+    parts.upload(rec)
+    api.step(ctx, parts, m, pbl, prm, wet_cells=wet)
+    g = parts.download()
+    st = orc.State.from_records(rec)
+    opbl = orc.pbl_diagnostics(frames[fa]["surface"], frames[fb]["surface"], alpha, spec.nx, spec.ny)
+    lam, frac = orc.wet_cells(precip, np.zeros(spec.nx * spec.ny), np.ones(spec.nx * spec.ny), scn.wet_a,
+                              scn.wet_b)
+    orc.step(st, n, met, opbl, prm, wet_cells_lf=(lam, frac), wet_shape=(spec.nx, spec.ny))
+    o = st.to_records()
+    act = (rec["flags"] & 1) != 0
+    f64 = lambda a: np.asarray(a, np.float64)[act]                     # noqa: E731
+    gx = lambda r, c, p: f64(r[c]) + f64(r[p])                          # noqa: E731
+    zsc = np.maximum(np.maximum(np.abs(f64(o["pos_z"])), np.abs(f64(rec["pos_z"]))), 100.0)
+    err = {"grid_x": np.abs(gx(g, "cell_x", "pos_x") - gx(o, "cell_x", "pos_x")),
+           "grid_y": np.abs(gx(g, "cell_y", "pos_y") - gx(o, "cell_y", "pos_y")),
+           "pos_z": np.abs(f64(g["pos_z"]) - f64(o["pos_z"])) / zsc}
+    for f in ("turb_u", "turb_v", "turb_w", "vel_u", "vel_v", "vel_w"):
+        err[f] = np.abs(f64(g[f]) - f64(o[f])) / np.maximum(np.abs(f64(o[f])), 2.0)
+    mo = f64(o["mass"][:, 0])
+    err["mass0"] = np.abs(f64(g["mass"][:, 0]) - mo) / np.maximum(np.abs(mo), 1e-30)
+    out = {k: float(v.max()) for k, v in err.items()}
+    within = {k: float((v <= 1e-5).mean()) for k, v in err.items()}
+    return {"particles": int(act.sum()), "max_rel_err": out, "share_within_1e-5": within,
+            "integers_bit_exact": bool(np.array_equal(g["flags"], o["flags"]) and np.array_equal(g["cbt"], o["cbt"])),
+            "step": "one production step (dry + per-cell wet) of the sample, device fused_step_kernel vs FP32 oracle"}
+
+
 def cpu_sample(scn, args, n):
     """A sample of particles in the plumes around the sources (no GPU)."""
     from flexpart_gpu import synthetic
@@ -241,6 +390,7 @@ def run_reference(args, rank, world):
     times = oracle_steps(scn, frames, rec, threads, steps=args.warmup + args.steps)[args.warmup:]
     total = sum(times)
     value = sample * len(times) / total
+    extra = cpu_figures(scn, frames, rec[:200_000], threads)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
@@ -250,7 +400,8 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{sample} plume particles per step, production step (4 sub-steps, reflection, "
                                    f"dual-time wind, dry + wet) of the oracle C restatement with {threads} OpenMP "
-                                   f"threads; the reference's CPU path is Rust and no Rust toolchain is present"},
+                                   f"threads; the reference's CPU path is Rust and no Rust toolchain is present",
+                         **extra},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -584,6 +735,36 @@ def run_cbl_convection(ctx, stream, parts, pbl, n_active, peak, args, rank, worl
     return out
 
 
+def profile_case(name):
+    """Small self-contained runs of the batched and inversion kernels for
+    profilers: inputs larger than L2, a few GB on the device at most, each
+    kernel launched a few dozen times."""
+    from flexpart_gpu import api, synthetic
+
+    ctx = api.Context(0)
+    if name == "batched":
+        from flexpart_gpu import batch as bt
+
+        ens = synthetic.config2(n_scenarios=64, lo=10_000, hi=200_000, hours=12)
+        b = bt.Batch(ctx, bt.ensemble_config(ens, output_every_steps=12), bt.ensemble_scenarios(ens),
+                     (ens.met.nx, ens.met.ny, ens.met.nz), synthetic.level_heights(ens.met.nz, ens.met.top_m),
+                     ens.outheights)
+        bt.upload_ensemble_met(b, ens)
+        b.run(ens.n_steps)
+        ctx.synchronize()
+        print("batched", ens.total_particles, "particles", ens.n_steps, "steps, errors", b.errors())
+    else:
+        from flexpart_gpu.adjoint import SourceInversion, misfit
+
+        inv = synthetic.config3(n_particles=200_000, hours=6)
+        inv.checkpoint_every = 0
+        model = SourceInversion(ctx, inv)
+        sim = model.forward(model.mass0, model.position0)
+        loss, d = misfit(sim, sim * 1.1 + 1e-12)
+        g = model.backward(d)
+        print("inverse loss", loss, "grad mass norm", float(np.linalg.norm(g["mass"])))
+
+
 def api_device(ctx, n, dtype):
     from flexpart_gpu import api
     return api.DeviceArray(ctx, n, dtype)
@@ -597,6 +778,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.case:
+        profile_case(args.case)
         return
 
     import ctypes
@@ -850,7 +1034,9 @@ def main():
         times = oracle_steps(scn, frames, rec, threads, seconds=10.0)
         cpu = {"value": sample * len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"the first {sample} particles of the spun-up population x {len(times)} production steps "
-                         f"(oracle C restatement, {threads} OpenMP threads, {sum(times):.1f} s)"}
+                         f"(oracle C restatement, {threads} OpenMP threads, {sum(times):.1f} s)",
+               "parity": parity_sample(ctx, scn, frames, rec, scn.end, [0, 0, 0, 0]),
+               **cpu_figures(scn, frames, rec, threads)}
 
     batched = None
     if not args.no_batched and not args.quick:

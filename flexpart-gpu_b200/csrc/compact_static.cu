@@ -28,6 +28,10 @@
 // address is looked up with cudaGetSymbolAddress once per device (with that
 // device current) on the first call made for a context on that device, and
 // cached.  That first call should therefore come before any stream capture.
+// The cached address belongs to the device's primary context as it was at
+// that first call: a cudaDeviceReset on that device ends the context and the
+// module with it, and this entry point must not be called again in that
+// process after such a reset.
 #include <cuda_runtime.h>
 
 #include <mutex>

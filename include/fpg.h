@@ -455,7 +455,9 @@ fpg_status fpg_sort_by_cell(fpg_ctx* ctx, fpg_particles* particles, const fpg_me
  * The first call for a device looks up the scratch array's device address
  * (once per device) and should come before any stream capture.  All calls
  * on a device share the one array: calls that overlap on the GPU race;
- * calls ordered on one stream are safe. */
+ * calls ordered on one stream are safe.  The looked-up address does not
+ * survive a cudaDeviceReset of that device: do not call this entry point
+ * again in a process after such a reset. */
 fpg_status fpg_compaction_indices_static(fpg_ctx* ctx, const uint32_t* flags_dev, size_t n,
                                          uint32_t* indices_dev, uint32_t* active_count_dev,
                                          void* stream);

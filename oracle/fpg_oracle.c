@@ -321,6 +321,16 @@ void orc_wet_cells_grid(size_t n, const float* lsp, const float* convp, const fl
                      &fraction_out[c]);
 }
 
+/* interpolate_wind_field_linear's per-value lerp (io/temporal.rs:67-120,
+ * 417-420: a.mul_add(1 - t, b * t)) over n values, as the reference's CPU
+ * pipeline time-interpolates a whole wind component before advecting
+ * (benches/advection.rs:1138-1146). */
+void orc_lerp_field(size_t n, const float* a, const float* b, float t, float* out, int n_threads) {
+    const float s = 1.0f - t;
+#pragma omp parallel for schedule(static) num_threads(n_threads > 0 ? n_threads : 1)
+    for (long long i = 0; i < (long long)n; ++i) out[i] = fmaf(a[i], s, b[i] * t);
+}
+
 /* ---- CBL skewed vertical-velocity PDF (physics/cbl.rs) ------------------
  * pdf[11] = updraft weight, mean, sigma; downdraft weight, mean, sigma;
  * target w2, w3, skewness; transition; z/h.  f32 throughout, as the CPU

@@ -318,6 +318,17 @@ def wet_cells(lsp, convp, cc, a, b):
     return lam, fr
 
 
+def lerp_field(a, b, t, threads=0):
+    """Whole-field time lerp of the reference's CPU pipeline
+    (interpolate_wind_field_linear, io/temporal.rs:67-120)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    out = np.empty_like(a)
+    lib.orc_lerp_field(ctypes.c_size_t(a.size), _ptr(a), _ptr(b), ctypes.c_float(t), _ptr(out),
+                       ctypes.c_int(threads or (os.cpu_count() or 1)))
+    return out
+
+
 # ---- grid functions --------------------------------------------------------
 
 class Pbl:
@@ -353,9 +364,11 @@ def pbl_diagnostics(surface_t0, surface_t1, alpha, nx, ny, options=None, dtype=n
 
 def step(state: State, n, met, pbl: Pbl, params: StepParams, wet_cells_lf=None, wet_shape=None,
          threads=0, dry_velocity=None, wet_lambda=None, wet_fraction=None,
-         dry_prob=None, wet_prob=None, wind_bias=None):
+         dry_prob=None, wet_prob=None, wind_bias=None, rng_index=None):
     """The fused production step over slots [0, n).  `met` is a dict with
-    u0, v0, w0, u1, v1, w1 ((nx, ny, nz) float32) and heights (nz,)."""
+    u0, v0, w0, u1, v1, w1 ((nx, ny, nz) float32) and heights (nz,).
+    `rng_index` (uint32, n) gives each slot's Philox block index when the
+    state is a sample of a larger population (default: the slot itself)."""
     u0 = np.ascontiguousarray(met["u0"], np.float32)
     nx, ny, nz = u0.shape
     arrs = [u0] + [np.ascontiguousarray(met[k], np.float32) for k in ("v0", "w0", "u1", "v1", "w1")]
@@ -384,11 +397,13 @@ def step(state: State, n, met, pbl: Pbl, params: StepParams, wet_cells_lf=None, 
     pc = pbl.cstruct() if pbl is not None else (_PblF64 if state.dtype == np.float64 else _PblF32)()
     bias = None if wind_bias is None else np.ascontiguousarray(wind_bias, np.float64).reshape(-1)
     assert bias is None or bias.size == 3 * nx * ny * nz
-    getattr(lib, "orc_step_biased" + _sfx(state.dtype))(
+    idx = None if rng_index is None else np.ascontiguousarray(rng_index, np.uint32)
+    assert idx is None or idx.size >= n
+    getattr(lib, "orc_step_indexed" + _sfx(state.dtype))(
         ctypes.byref(st), ctypes.c_size_t(n), *[_ptr(a) for a in arrs],
         ctypes.c_size_t(nx), ctypes.c_size_t(ny), ctypes.c_size_t(nz), _ptr(hts),
         ctypes.byref(pc), ctypes.byref(prm), _ptr(lam), _ptr(fr),
-        ctypes.c_size_t(wnx), ctypes.c_size_t(wny), ctypes.c_int(threads), _ptr(bias))
+        ctypes.c_size_t(wnx), ctypes.c_size_t(wny), ctypes.c_int(threads), _ptr(bias), _ptr(idx))
 
 
 def level_of(z, outheights, dtype=np.float32):

@@ -54,6 +54,10 @@ def _fields(rec_or_state):
 
 
 ENVELOPE = 4.0
+# Largest share of the active particles a floating-point field may pass
+# through the FP64 envelope alone (below one particle in 10 000; none in a
+# population of fewer than 10 000 active particles).
+MAX_ENVELOPE_SHARE = 1e-4
 
 
 def field_checks(g, s, z_in, s64=None, stats=None):
@@ -84,6 +88,47 @@ def field_checks(g, s, z_in, s64=None, stats=None):
                 stats[f] = stats.get(f, 0) + int((~ok & env).sum())
             ok = ok | env
         out[f] = ok
+    return out
+
+
+def assert_parity(g, s, z_in, s64, label, n_active=None, max_share=MAX_ENVELOPE_SHARE):
+    """Every floating-point field within tolerance (field_checks), at most
+    `max_share` of the active particles passing through the FP64 envelope
+    per field, and the integer fields (flags, cbt) bit-exact.  Returns the
+    envelope counts per field."""
+    stats = {}
+    checks = field_checks(g, s, z_in, s64, stats)
+    for k, ok in checks.items():
+        if not ok.all():
+            bad = np.flatnonzero(~ok)[:5]
+            detail = [(int(i), float(z_in[i]), float(g["pos_z"][i]), float(np.asarray(s.pos_z)[i]),
+                       float(g["turb_w"][i]), float(np.asarray(s.turb_w)[i])) for i in bad]
+            raise AssertionError(f"{label}: {k} differs at (slot, z_in, z_gpu, z_orc, tw_gpu, tw_orc) {detail}")
+    if n_active is None:
+        n_active = int((np.asarray(s.flags) & 1).sum())
+    allowed = int(np.floor(max_share * n_active))
+    over = {k: v for k, v in stats.items() if v > allowed}
+    assert not over, f"{label}: envelope share above {max_share} of {n_active} active particles: {over}"
+    assert np.array_equal(g["flags"], np.asarray(s.flags)), f"{label}: flags"
+    assert np.array_equal(g["cbt"], np.asarray(s.cbt)), f"{label}: cbt"
+    return stats
+
+
+FP64_FIELDS = ("grid_x", "grid_y", "pos_z", "turb_u", "turb_v", "turb_w", "mass0")
+
+
+def fp64_errors(g, s, s64, z_in, active):
+    """Max scaled error against the FP64 oracle of the GPU and of the FP32
+    oracle, per field, over the active particles (scales as field_checks:
+    1 cell, the height scale, 2 m/s, the mass itself)."""
+    G, S, D = _fields(g), _fields(s), _fields(s64)
+    zs = np.maximum(np.maximum(np.abs(D["pos_z"][active]), np.abs(z_in[active].astype(np.float64))), 100.0)
+    floors = {"grid_x": 1.0, "grid_y": 1.0, "turb_u": 2.0, "turb_v": 2.0, "turb_w": 2.0, "mass0": 1e-30}
+    out = {}
+    for f in FP64_FIELDS:
+        ref = D[f][active]
+        sc = zs if f == "pos_z" else np.maximum(np.abs(ref), floors[f])
+        out[f] = (float(np.max(np.abs(G[f][active] - ref) / sc)), float(np.max(np.abs(S[f][active] - ref) / sc)))
     return out
 
 

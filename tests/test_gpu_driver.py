@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from flexpart_gpu import synthetic
-from helpers import field_checks
+from helpers import assert_parity
 from oracle.forward import OracleForward
 
 pytestmark = pytest.mark.gpu
@@ -67,9 +67,7 @@ def test_driver_steps_match_oracle_loop(ctx, mode):
             o = fw.records()
             # heights at the step start (release height for particles released this step)
             z_in = np.where(z_prev == 0.0, o["pos_z"], z_prev)
-            for name, ok in field_checks(g, fw.state, z_in, fw64.state).items():
-                assert ok.all(), (mode, k, name, np.flatnonzero(~ok)[:5])
-            assert np.array_equal(g["flags"], o["flags"])
+            assert_parity(g, fw.state, z_in, fw64.state, f"{mode} step {k}")
             assert np.array_equal(g["release_point"], o["release_point"])
             assert np.array_equal(g["time"], o["time"])
 

@@ -9,7 +9,8 @@ larger than the FP32 oracle's own (both printed).
 import numpy as np
 import pytest
 
-from helpers import close, field_checks, oracle_step, pbl_arrays, population, production_params, small_met
+from helpers import (assert_parity, close, fp64_errors, oracle_step, pbl_arrays, population, production_params,
+                     small_met)
 from oracle import orc
 
 pytestmark = pytest.mark.gpu
@@ -40,18 +41,9 @@ def _gpu_setup(ctx, spec, frames, met, alpha, rec):
 
 
 def _compare_state(g, s, label, rec_in, s64=None):
-    stats = {}
-    checks = field_checks(g, s, rec_in["pos_z"], s64, stats)
+    stats = assert_parity(g, s, rec_in["pos_z"], s64, label)
     if any(stats.values()):
         print(f"{label}: particles held to the FP32 envelope: {stats}")
-    for k, ok in checks.items():
-        if not ok.all():
-            bad = np.flatnonzero(~ok)[:5]
-            detail = [(int(i), float(rec_in["pos_z"][i]), float(g["pos_z"][i]), float(s.pos_z[i]),
-                       float(g["turb_w"][i]), float(s.turb_w[i])) for i in bad]
-            raise AssertionError(f"{label}: {k} differs at (slot, z_in, z_gpu, z_orc, tw_gpu, tw_orc) {detail}")
-    assert np.array_equal(g["flags"], s.flags), f"{label}: flags"
-    assert np.array_equal(g["cbt"], s.cbt), f"{label}: cbt"
 
 
 def test_philox_kernel_bit_exact(ctx):
@@ -109,19 +101,7 @@ def test_fused_step_one_step_matches_oracle(ctx, n):
     act = rec["flags"] == 1
     if not act.any():
         return
-    zs = np.maximum(np.maximum(np.abs(s64.pos_z[act]), np.abs(rec["pos_z"][act])), 100.0)
-    gx = lambda cx, px: cx.astype(np.float64) + px                     # noqa: E731
-    fields = (("grid_x", gx(g["cell_x"], g["pos_x"]), gx(s.cell_x, s.pos_x), gx(s64.cell_x, s64.pos_x), 1.0),
-              ("grid_y", gx(g["cell_y"], g["pos_y"]), gx(s.cell_y, s.pos_y), gx(s64.cell_y, s64.pos_y), 1.0),
-              ("pos_z", g["pos_z"], s.pos_z, s64.pos_z, None),
-              ("turb_u", g["turb_u"], s.turb_u, s64.turb_u, 2.0), ("turb_v", g["turb_v"], s.turb_v, s64.turb_v, 2.0),
-              ("turb_w", g["turb_w"], s.turb_w, s64.turb_w, 2.0),
-              ("mass0", g["mass"][:, 0], s.mass[0], s64.mass[0], 1e-30))
-    for name, a, b, c, floor in fields:
-        ref = np.asarray(c, np.float64)[act]
-        sc = zs if floor is None else np.maximum(np.abs(ref), floor)
-        e_gpu = np.max(np.abs(np.asarray(a, np.float64)[act] - ref) / sc)
-        e_orc = np.max(np.abs(np.asarray(b, np.float64)[act] - ref) / sc)
+    for name, (e_gpu, e_orc) in fp64_errors(g, s, s64, rec["pos_z"], act).items():
         print(f"n={n}: max scaled |{name} - fp64|: gpu {e_gpu:.2e}, oracle f32 {e_orc:.2e}")
         assert e_gpu <= 2.0 * e_orc + 1e-6, name
 

@@ -47,3 +47,24 @@ def test_forward_loop_alpha_sequence_of_reference_test():
     # tests/forward_timeloop.rs:100-126: bracket [t0, t0+2], dt 1 -> alpha 0, 0.5, 1
     for k, a in enumerate([0.0, 0.5, 1.0]):
         assert orc.interpolation_alpha(10, 12, 10 + k) == (0, a)
+
+
+def test_sampled_step_with_slot_indices_equals_population_step():
+    """orc.step on a sample of slots, each keeping its Philox index through
+    rng_index, gives the same bits as the step of the whole population at
+    those slots (the sampled parity tests at full size rely on it)."""
+    from helpers import oracle_step, pbl_arrays, population, production_params, small_met
+
+    spec, frames, met = small_met()
+    rec = population(spec.nx, spec.ny, 3000, seed=4)
+    prm = production_params(alpha=0.6, counter=(11, 0, 0, 0))
+    pbl = pbl_arrays(frames, 0.6, spec.nx, spec.ny)
+    full = oracle_step(rec, met, pbl, prm).to_records()
+    slots = np.sort(np.random.default_rng(1).choice(3000, 400, replace=False)).astype(np.uint32)
+    st = orc.State.from_records(rec[slots])
+    orc.step(st, len(slots), met, pbl, prm, rng_index=slots)
+    assert st.to_records().tobytes() == full[slots].tobytes()
+    # without the indices the sample draws other noise
+    st2 = orc.State.from_records(rec[slots])
+    orc.step(st2, len(slots), met, pbl, prm)
+    assert st2.to_records().tobytes() != full[slots].tobytes()

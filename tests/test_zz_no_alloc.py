@@ -41,25 +41,59 @@ def _existing(ctx, flags):
     return idx.numpy()[:count], count
 
 
-def _static(ctx, flags):
+def _buffers(ctx, flags):
+    """Device input and output buffers of one call (uploaded, synchronised)."""
     n = len(flags)
-    d_flags = api.DeviceArray.from_numpy(ctx, flags)
-    d_idx = api.DeviceArray(ctx, n, np.uint32)
-    d_cnt = api.DeviceArray(ctx, 1, np.uint32)
-    st = api._lib.lib.fpg_compaction_indices_static(ctx.h, ctypes.c_void_p(d_flags.ptr), n,
+    return (api.DeviceArray.from_numpy(ctx, flags), api.DeviceArray(ctx, n, np.uint32),
+            api.DeviceArray(ctx, 1, np.uint32))
+
+
+def _enqueue(ctx, bufs):
+    """Queues one call on the context's stream, with no host synchronisation."""
+    d_flags, d_idx, d_cnt = bufs
+    st = api._lib.lib.fpg_compaction_indices_static(ctx.h, ctypes.c_void_p(d_flags.ptr), d_flags.n,
                                                     ctypes.c_void_p(d_idx.ptr), ctypes.c_void_p(d_cnt.ptr), None)
     assert st == 0, api._lib.lib.fpg_status_string(st)
-    ctx.synchronize()
+    return bufs
+
+
+def _result(bufs):
+    _, d_idx, d_cnt = bufs
     count = int(d_cnt.numpy()[0])
     return d_idx.numpy()[:count], count
 
 
+def _static(ctx, flags):
+    bufs = _enqueue(ctx, _buffers(ctx, flags))
+    ctx.synchronize()
+    return _result(bufs)
+
+
 def test_static_scan_matches_fpg_compact_twice():
     ctx = api.Context(0)
-    for n, seed, density in ((300_001, 1, 0.9), (70_000, 2, 0.3)):
+    # 3,000,001 slots are 1465 tiles: the single-CTA scan then runs two tiles
+    # per thread with a shorter range on the last busy thread
+    for n, seed, density in ((300_001, 1, 0.9), (70_000, 2, 0.3), (3_000_001, 3, 0.55)):
         flags = _flags(n, seed, density)
         ref_idx, ref_count = _existing(ctx, flags)
         idx, count = _static(ctx, flags)
+        assert count == ref_count == int(flags.sum())
+        assert np.array_equal(idx, ref_idx)
+
+
+def test_static_scan_back_to_back_on_one_stream():
+    """Two calls queued on one stream with no host synchronisation between
+    them share the scratch array in turn; each result matches fpg_compact."""
+    ctx = api.Context(0)
+    fa = _flags(2_500_003, 4, 0.2)
+    fb = _flags(400_000, 5, 0.8)
+    a, b = _buffers(ctx, fa), _buffers(ctx, fb)
+    _enqueue(ctx, a)
+    _enqueue(ctx, b)
+    ctx.synchronize()
+    for flags, bufs in ((fa, a), (fb, b)):
+        ref_idx, ref_count = _existing(ctx, flags)
+        idx, count = _result(bufs)
         assert count == ref_count == int(flags.sum())
         assert np.array_equal(idx, ref_idx)
 
