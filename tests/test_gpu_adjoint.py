@@ -46,6 +46,20 @@ def _problem(hours, smooth, n_particles=16_000, n_sources=4, K=3):
     return inv
 
 
+def _problem_c3(hours=4, n_particles=32_000, K=8):
+    """The source inversion's own shape: 16 sources released over 6 h from a
+    step in the first half of the run, 200 random receptor cells of the
+    lowest layer, full physics (PBL per cell, dry deposition), checkpoints
+    every K steps; fewer particles and a shorter horizon than the 1 M-particle
+    24 h run, so that central differences of the FP64 map stay affordable and
+    no particle leaves the linear range of the steps.  Receptors are sampled
+    every step."""
+    inv = synthetic.config3(n_particles=n_particles, n_sources=16, n_receptors=200, hours=hours)
+    inv.sample_every = 1
+    inv.checkpoint_every = K
+    return inv
+
+
 def _obs(sim, seed=1):
     rng = np.random.default_rng(seed)
     return sim * (1.0 + 0.3 * rng.standard_normal(sim.size))
@@ -181,11 +195,16 @@ def test_short_horizon_gradients_match_device_finite_differences(ctx):
         assert np.linalg.norm(ga - fd) <= 2e-2 * np.linalg.norm(fd), kind
 
 
-@pytest.mark.parametrize("hours,smooth", [(1, True), (3, True), (3, False)])
-def test_gradients_match_the_fp64_reference_gradient(ctx, hours, smooth):
+@pytest.mark.parametrize("hours,smooth,shape", [(1, True, "grid"), (3, True, "grid"), (3, False, "grid"),
+                                                (4, False, "c3")])
+def test_gradients_match_the_fp64_reference_gradient(ctx, hours, smooth, shape):
+    """Every gradient type within 1e-3 relative (in norm) of the FP64
+    reference gradient: all masses, all positions, and 40 wind-bias entries
+    (the 10 largest of each component and 10 drawn at random among the
+    non-zero ones)."""
     from oracle.inverse import OracleInversion
 
-    inv = _problem(hours, smooth)
+    inv = _problem(hours, smooth) if shape == "grid" else _problem_c3(hours)
     model = adj.SourceInversion(ctx, inv)
     sim = model.forward(model.mass0, model.position0)
     obs = _obs(sim)
@@ -219,7 +238,9 @@ def test_gradients_match_the_fp64_reference_gradient(ctx, hours, smooth):
             pm[s, c] -= h
             ref_p[s, c] = (loss(p=pp) - loss(p=pm)) / (2 * h)
     gb = g["wind_bias"].reshape(-1)
-    idx = _top_bias(gb, per_comp=3)
+    idx = _top_bias(gb, per_comp=10)
+    rest = np.setdiff1d(np.flatnonzero(gb != 0.0), idx)
+    idx += [int(i) for i in np.random.default_rng(7).choice(rest, min(10, len(rest)), replace=False)]
     ref_b = []
     for i in idx:
         b = np.zeros(gb.size)
@@ -231,9 +252,10 @@ def test_gradients_match_the_fp64_reference_gradient(ctx, hours, smooth):
     e_m = np.linalg.norm(g["mass"] - ref_m) / np.linalg.norm(ref_m)
     e_p = np.linalg.norm(g["position"] - ref_p) / np.linalg.norm(ref_p)
     e_b = np.linalg.norm(gb[idx] - ref_b) / np.linalg.norm(ref_b)
-    print(f"hours {hours} smooth {smooth}: rel error mass {e_m:.2e} position {e_p:.2e} bias {e_b:.2e}")
+    print(f"{shape} hours {hours} smooth {smooth}: rel error mass {e_m:.2e} position {e_p:.2e} bias {e_b:.2e} "
+          f"({len(idx)} bias entries)")
     print("position adjoint", g["position"].ravel(), "fp64", ref_p.ravel())
     print("bias adjoint", gb[idx], "fp64", ref_b)
     assert e_m <= 1e-3
-    assert e_p <= 3e-2
-    assert e_b <= 3e-2
+    assert e_p <= 1e-3
+    assert e_b <= 1e-3
