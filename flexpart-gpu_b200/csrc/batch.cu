@@ -85,12 +85,13 @@ __global__ void __launch_bounds__(256) batch_pack_kernel(const BatchState* st, c
 __global__ void __launch_bounds__(256) batch_pbl_kernel(const BatchState* st, const fpg_surface_cell* __restrict__ sring,
                                                         const float* __restrict__ precip, fpg_pbl_options o,
                                                         uint32_t ncell, float* f0, float* f1, float* f2, float* f3,
-                                                        float* f4, float* f5, float* f6, float4* packed, int wet_on,
+                                                        float* f4, float* f5, float* f6, float4* packed,
+                                                        CellHanna* hanna, int wet_on,
                                                         float wa, float wb, float2* wet) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     pbl_cell(sring + (size_t)st->fa * ncell, sring + (size_t)st->fb * ncell, st->alpha, o, c, f0, f1, f2, f3, f4, f5,
-             f6, packed);
+             f6, packed, hanna);
     if (wet_on && st->changed) wet[c] = wet_cell_forcing(precip[(size_t)st->fa * ncell + c], 0.0f, 1.0f, wa, wb);
 }
 
@@ -281,7 +282,7 @@ StepArgs make_step_args(fpg_batch* b) {
     a.monotonic = b->met->monotonic;
     a.dt = (float)c.timestep_seconds;
     a.xs = c.x_grid_per_meter; a.ys = c.y_grid_per_meter; a.zs = c.z_grid_per_meter;
-    a.pbl = b->pbl->packed;
+    a.hcell = b->pbl->hanna;
     a.pnx = (uint32_t)b->pbl->nx; a.pny = (uint32_t)b->pbl->ny;
     a.tdt = (float)c.timestep_seconds;
     a.rho = c.rho_grad_over_rho;
@@ -343,7 +344,7 @@ void enqueue_pre(fpg_batch* b, cudaStream_t s) {
     batch_pack_kernel<<<b->ctx->sm_count * 4, 256, 0, s>>>(b->st, b->ring, nodes, b->met->bracket);
     batch_pbl_kernel<<<(cells + 255) / 256, 256, 0, s>>>(
         b->st, b->sring, b->pring, b->cfg.pbl_options, cells, b->pbl->field[0], b->pbl->field[1], b->pbl->field[2],
-        b->pbl->field[3], b->pbl->field[4], b->pbl->field[5], b->pbl->field[6], b->pbl->packed,
+        b->pbl->field[3], b->pbl->field[4], b->pbl->field[5], b->pbl->field[6], b->pbl->packed, b->pbl->hanna,
         b->cfg.wet_from_precipitation, b->cfg.wet_gas_a, b->cfg.wet_gas_b, b->wet ? b->wet->lf : nullptr);
     batch_release_kernel<<<dim3(16, (unsigned)b->scen.size()), 256, 0, s>>>(b->st, b->sc, c, pop_fields(b));
     b->ctx->count(4);

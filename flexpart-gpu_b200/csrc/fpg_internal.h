@@ -12,6 +12,8 @@
 
 namespace fpg {
 
+struct CellHanna;  // physics.cuh: the per-cell Hanna constants (48 bytes)
+
 // Records the CUDA error for fpg_last_cuda_error() and maps it to a status.
 fpg_status cuda_status(cudaError_t e);
 
@@ -65,6 +67,7 @@ struct fpg_pbl {
     size_t nx = 0, ny = 0;
     float* field[7] = {};                   // ustar, wstar, hmix, oli, sshf, ssr, surfstr
     float4* packed = nullptr;               // (ustar, wstar, hmix, oli) per cell
+    fpg::CellHanna* hanna = nullptr;        // the Hanna constants of each cell (the fused step reads these)
     bool ready = false;
 };
 

@@ -120,64 +120,176 @@ __device__ __forceinline__ int hanna_regime(float ol, float h) {
                                                                : REGIME_STABLE;
 }
 
+// ---- per-cell Hanna constants -----------------------------------------------
+// What compute_hanna and hanna_short_w derive from a met cell's PBL
+// parameters alone, computed once per cell (pbl_cell) instead of up to four
+// times per particle-step: the floored u*, w*, h (hanna.rs:50-53), the
+// Obukhov length, the stability regime, and per regime
+//   * the leading constant factors of the reference's products, which C++
+//     evaluates left to right (1.2f * wst * wst * (1 - 0.9 zeta) * z23
+//     rounds (1.2f * wst) * wst first), so the per-cell product is the same
+//     float the per-particle expression forms;
+//   * the outputs that depend on the cell only, floored and sanitised as
+//     compute_hanna does: sigma_u = sigma_v and T_Lu = T_Lv of the unstable
+//     branch (hanna.rs:81-86, 120-131), dsigma_w/dz of the stable branch
+//     (hanna.rs:106).
+// Same operations in the same order: the per-particle results are bit for
+// bit those of evaluating everything per particle.
+//   neutral:  k0 = 2 u*,  k1 = 1.3 u*
+//   unstable: k0 = sigma_u, k1 = T_Lu, k2 = 1.2 w* w*, k3 = -1.4 u* u*,
+//             k4 = w* w*, k5 = 0.15 h
+//   stable:   k0 = 2 u*,  k1 = 1.3 u*, k2 = dsigma_w/dz, k5 = 0.15 h, k6 = 0.1 h
+struct __align__(16) CellHanna {
+    float ust, wst, h, ol;
+    float k0, k1, k2, k3;
+    float k4, k5, k6;
+    int regime;
+};
+
+// The constants of `regime` for a cell (ust, wst, h unfloored; ol = L).
+__device__ __forceinline__ CellHanna cell_hanna_for_regime(float ust_in, float wst_in, float ol, float h_in,
+                                                           int regime) {
+    CellHanna c;
+    c.ust = fmaxf(ust_in, 1.0e-4f);
+    c.wst = fmaxf(wst_in, 0.0f);
+    c.h = fmaxf(h_in, 1.0f);
+    c.ol = ol;
+    c.regime = regime;
+    c.k0 = c.k1 = c.k2 = c.k3 = c.k4 = c.k5 = c.k6 = 0.0f;
+    if (regime == REGIME_UNSTABLE) {
+        float sigu = 1.0e-2f + c.ust * pow_third(12.0f - 0.5f * c.h / ol);
+        float tlu = 0.15f * c.h / sigu;
+        tlu = fmaxf(tlu, 10.0f);
+        if (!finitef(sigu) || sigu <= 0.0f) sigu = 1.0e-2f;
+        if (!finitef(tlu)) tlu = 10.0f;
+        c.k0 = sigu;
+        c.k1 = tlu;
+        c.k2 = 1.2f * c.wst * c.wst;
+        c.k3 = -1.4f * c.ust * c.ust;
+        c.k4 = c.wst * c.wst;
+        c.k5 = 0.15f * c.h;
+    } else {
+        c.k0 = 2.0f * c.ust;
+        c.k1 = 1.3f * c.ust;
+        if (regime == REGIME_STABLE) {
+            float d = -1.3f * c.ust / c.h;
+            if (d == 0.0f) d = 1.0e-10f;
+            if (!finitef(d)) d = 1.0e-10f;
+            c.k2 = d;
+            c.k5 = 0.15f * c.h;
+            c.k6 = 0.1f * c.h;
+        }
+    }
+    return c;
+}
+
+// The constants of a cell's own regime (the branch test of hanna.rs:69-112
+// on the floored h).
+__device__ __forceinline__ CellHanna cell_hanna(float ust_in, float wst_in, float ol, float h_in) {
+    return cell_hanna_for_regime(ust_in, wst_in, ol, h_in, hanna_regime(ol, fmaxf(h_in, 1.0f)));
+}
+
+__device__ __forceinline__ CellHanna ld_cell_hanna(const CellHanna* p) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+    CellHanna c;
+    c.ust = a.x; c.wst = a.y; c.h = a.z; c.ol = a.w;
+    c.k0 = b.x; c.k1 = b.y; c.k2 = b.z; c.k3 = b.w;
+    c.k4 = d.x; c.k5 = d.y; c.k6 = d.z; c.regime = __float_as_int(d.w);
+    return c;
+}
+
+__device__ __forceinline__ void st_cell_hanna(CellHanna* p, const CellHanna& c) {
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(c.ust, c.wst, c.h, c.ol);
+    q[1] = make_float4(c.k0, c.k1, c.k2, c.k3);
+    q[2] = make_float4(c.k4, c.k5, c.k6, __int_as_float(c.regime));
+}
+
+// sigma_w, dsigma_w/dz, T_Lw of the unstable branch at height z
+// (hanna.rs:87-104,132-141, langevin_fused.wgsl:305-327).
 template <class T>
-__device__ __forceinline__ HannaT<T> compute_hanna_t(float ust_in, float wst_in, float ol, float h_in, T z_in) {
+__device__ __forceinline__ void hanna_unstable_w(const CellHanna& c, T z, T zeta, T& sigw, T& dsigwdz, T& tlw) {
+    const T cz = xcbrt(zeta);
+    const T z23 = cz * cz;
+    const T sigw_sq = c.k2 * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * c.ust * c.ust;
+    sigw = xsqrt(sigw_sq) + 1.0e-2f;
+    const T zm13 = 1.0f / (val(zeta) >= 1.0e-3f ? cz : T(pow_third(1.0e-3f)));
+    dsigwdz = 0.5f / sigw / c.h * (c.k3 + c.k4 * (0.8f * zm13 - 1.8f * z23));
+    if (val(z) < fabsf(c.ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * xabs(z / c.ol)));
+    else if (val(zeta) < 0.1f) tlw = 0.59f * z / sigw;
+    else tlw = c.k5 / sigw * (1.0f - xexp(-5.0f * zeta));
+}
+
+// compute_hanna_params (physics/hanna.rs:49-163) at height z_in of a cell.
+template <class T>
+__device__ __forceinline__ HannaT<T> compute_hanna_cell_t(const CellHanna& c, T z_in) {
     HannaT<T> o;
-    const float ust = fmaxf(ust_in, 1.0e-4f);
-    const float wst = fmaxf(wst_in, 0.0f);
-    const float h = fmaxf(h_in, 1.0f);
+    const float ust = c.ust, h = c.h;
     const T z = xclamp(z_in, 0.0f, h);
     const T zeta = xclamp(z / h, 0.0f, 1.0f);
     T sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
-    o.regime = hanna_regime(ol, h);
-    if (o.regime == REGIME_NEUTRAL) {
+    o.regime = c.regime;
+    if (c.regime == REGIME_NEUTRAL) {
         const T corr = z / ust;
-        sigu = 1.0e-2f + 2.0f * ust * xexp(-3.0e-4f * corr);
-        sigw = 1.3f * ust * xexp(-2.0e-4f * corr);
+        sigu = 1.0e-2f + c.k0 * xexp(-3.0e-4f * corr);
+        sigw = c.k1 * xexp(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
         sigv = sigw;
         tlu = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
         tlv = tlu;
         tlw = tlu;
-    } else if (o.regime == REGIME_UNSTABLE) {
-        sigu = T(1.0e-2f + ust * pow_third(12.0f - 0.5f * h / ol));
+        tlu = xmax(tlu, 10.0f);
+        tlv = xmax(tlv, 10.0f);
+        tlw = xmax(tlw, 30.0f);
+        if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
+        if (!finitef(val(sigu)) || val(sigu) <= 0.0f) sigu = T(1.0e-2f);
+        if (!finitef(val(sigv)) || val(sigv) <= 0.0f) sigv = T(1.0e-2f);
+        if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
+        if (!finitef(val(tlu))) tlu = T(10.0f);
+        if (!finitef(val(tlv))) tlv = T(10.0f);
+        if (!finitef(val(tlw))) tlw = T(30.0f);
+        if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
+    } else if (c.regime == REGIME_UNSTABLE) {
+        // sigma_u, sigma_v, T_Lu, T_Lv: the cell's, already final
+        sigu = T(c.k0);
         sigv = sigu;
-        const T c = xcbrt(zeta);
-        const T z23 = c * c;
-        const T sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
-        sigw = xsqrt(sigw_sq) + 1.0e-2f;
-        const T zm13 = 1.0f / (val(zeta) >= 1.0e-3f ? c : T(pow_third(1.0e-3f)));
-        dsigwdz = 0.5f / sigw / h * (-1.4f * ust * ust + wst * wst * (0.8f * zm13 - 1.8f * z23));
-        tlu = T(0.15f * h / val(sigu));
+        tlu = T(c.k1);
         tlv = tlu;
-        if (val(z) < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * xabs(z / ol)));
-        else if (val(zeta) < 0.1f) tlw = 0.59f * z / sigw;
-        else tlw = 0.15f * h / sigw * (1.0f - xexp(-5.0f * zeta));
+        hanna_unstable_w<T>(c, z, zeta, sigw, dsigwdz, tlw);
+        tlw = xmax(tlw, 30.0f);
+        if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
+        if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
+        if (!finitef(val(tlw))) tlw = T(30.0f);
+        if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
     } else {
-        sigu = 1.0e-2f + 2.0f * ust * (1.0f - zeta);
-        sigv = 1.0e-2f + 1.3f * ust * (1.0f - zeta);
+        sigu = 1.0e-2f + c.k0 * (1.0f - zeta);
+        sigv = 1.0e-2f + c.k1 * (1.0f - zeta);
         sigw = sigv;
-        dsigwdz = T(-1.3f * ust / h);
-        tlu = 0.15f * h / sigu * xsqrt(zeta);
+        dsigwdz = T(c.k2);                       // the cell's, already final
+        tlu = c.k5 / sigu * xsqrt(zeta);
         tlv = 0.467f * tlu;
-        tlw = 0.1f * h / sigw * xpow(zeta, 0.8f);
+        tlw = c.k6 / sigw * xpow(zeta, 0.8f);
+        tlu = xmax(tlu, 10.0f);
+        tlv = xmax(tlv, 10.0f);
+        tlw = xmax(tlw, 30.0f);
+        if (!finitef(val(sigu)) || val(sigu) <= 0.0f) sigu = T(1.0e-2f);
+        if (!finitef(val(sigv)) || val(sigv) <= 0.0f) sigv = T(1.0e-2f);
+        if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
+        if (!finitef(val(tlu))) tlu = T(10.0f);
+        if (!finitef(val(tlv))) tlv = T(10.0f);
+        if (!finitef(val(tlw))) tlw = T(30.0f);
     }
-    tlu = xmax(tlu, 10.0f);
-    tlv = xmax(tlv, 10.0f);
-    tlw = xmax(tlw, 30.0f);
-    if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
-    if (!finitef(val(sigu)) || val(sigu) <= 0.0f) sigu = T(1.0e-2f);
-    if (!finitef(val(sigv)) || val(sigv) <= 0.0f) sigv = T(1.0e-2f);
-    if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
-    if (!finitef(val(tlu))) tlu = T(10.0f);
-    if (!finitef(val(tlv))) tlv = T(10.0f);
-    if (!finitef(val(tlw))) tlw = T(30.0f);
-    if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
-    o.ust = ust; o.wst = wst; o.ol = ol; o.h = h;
+    o.ust = c.ust; o.wst = c.wst; o.ol = c.ol; o.h = c.h;
     o.sigu = sigu; o.sigv = sigv; o.sigw = sigw; o.dsigwdz = dsigwdz;
     o.tlu = tlu; o.tlv = tlv; o.tlw = tlw;
     return o;
+}
+
+template <class T>
+__device__ __forceinline__ HannaT<T> compute_hanna_t(float ust_in, float wst_in, float ol, float h_in, T z_in) {
+    return compute_hanna_cell_t<T>(cell_hanna(ust_in, wst_in, ol, h_in), z_in);
 }
 
 __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float ol, float h_in, float z_in) {
@@ -185,46 +297,43 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
 }
 
 // hanna_short_w (langevin_fused.wgsl:296-344): sigw, dsigwdz, tlw at a new
-// height.  ust, wst, h are the already-floored values of compute_hanna.
-// The branch test of the shader (`!finite(ol) || ol == 0 || h/|ol| < 1`,
-// then `ol < 0`) sees the same floored h and the same ol as compute_hanna's
-// for this particle, so its outcome is the `regime` compute_hanna found.
+// height in a cell.  The shader's branch test (`!finite(ol) || ol == 0 ||
+// h/|ol| < 1`, then `ol < 0`) sees the same floored h and the same ol as
+// compute_hanna's for this particle, so its outcome is the cell's regime.
 template <class T>
-__device__ __forceinline__ void hanna_short_w_t(float ust_in, float wst_in, float ol, float h_in, T z_in, int regime,
-                                                T& sigw_o, T& dsigwdz_o, T& tlw_o) {
-    const float ust = fmaxf(ust_in, 1.0e-4f);
-    const float wst = fmaxf(wst_in, 0.0f);
-    const float h = fmaxf(h_in, 1.0f);
-    const T z = xclamp(z_in, 0.0f, h);
-    const T zeta = xclamp(z / h, 0.0f, 1.0f);
+__device__ __forceinline__ void hanna_short_cell_t(const CellHanna& c, T z_in, T& sigw_o, T& dsigwdz_o, T& tlw_o) {
+    const T z = xclamp(z_in, 0.0f, c.h);
+    const T zeta = xclamp(z / c.h, 0.0f, 1.0f);
     T sigw, dsigwdz, tlw;
-    if (regime == REGIME_NEUTRAL) {
-        const T corr = z / ust;
-        sigw = 1.3f * ust * xexp(-2.0e-4f * corr);
+    if (c.regime == REGIME_NEUTRAL) {
+        const T corr = z / c.ust;
+        sigw = c.k1 * xexp(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
         tlw = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
-    } else if (regime == REGIME_UNSTABLE) {
-        const T c = xcbrt(zeta);
-        const T z23 = c * c;
-        const T sigw_sq = 1.2f * wst * wst * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * ust * ust;
-        sigw = xsqrt(sigw_sq) + 1.0e-2f;
-        const T zm13 = 1.0f / (val(zeta) >= 1.0e-3f ? c : T(pow_third(1.0e-3f)));
-        dsigwdz = 0.5f / sigw / h * (-1.4f * ust * ust + wst * wst * (0.8f * zm13 - 1.8f * z23));
-        if (val(z) < fabsf(ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * xabs(z / ol)));
-        else if (val(zeta) < 0.1f) tlw = 0.59f * z / sigw;
-        else tlw = 0.15f * h / sigw * (1.0f - xexp(-5.0f * zeta));
+    } else if (c.regime == REGIME_UNSTABLE) {
+        hanna_unstable_w<T>(c, z, zeta, sigw, dsigwdz, tlw);
     } else {
-        sigw = 1.0e-2f + 1.3f * ust * (1.0f - zeta);
-        dsigwdz = T(-1.3f * ust / h);
-        tlw = 0.1f * h / sigw * xpow(zeta, 0.8f);
+        sigw = 1.0e-2f + c.k1 * (1.0f - zeta);
+        dsigwdz = T(c.k2);                       // the cell's, already final
+        tlw = c.k6 / sigw * xpow(zeta, 0.8f);
     }
     tlw = xmax(tlw, 30.0f);
-    if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
+    if (c.regime != REGIME_STABLE) {
+        if (val(dsigwdz) == 0.0f) dsigwdz = T(1.0e-10f);
+        if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
+    }
     if (!finitef(val(sigw)) || val(sigw) <= 0.0f) sigw = T(1.0e-2f);
     if (!finitef(val(tlw))) tlw = T(30.0f);
-    if (!finitef(val(dsigwdz))) dsigwdz = T(1.0e-10f);
     sigw_o = sigw; dsigwdz_o = dsigwdz; tlw_o = tlw;
+}
+
+// The same from a cell's raw parameters with the branch given by the caller
+// (ust, wst, h floored here, as hanna_short_w receives them).
+template <class T>
+__device__ __forceinline__ void hanna_short_w_t(float ust_in, float wst_in, float ol, float h_in, T z_in, int regime,
+                                                T& sigw_o, T& dsigwdz_o, T& tlw_o) {
+    hanna_short_cell_t<T>(cell_hanna_for_regime(ust_in, wst_in, ol, h_in, regime), z_in, sigw_o, dsigwdz_o, tlw_o);
 }
 
 __device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float ol, float h_in, float z_in,

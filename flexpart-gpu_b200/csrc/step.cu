@@ -56,17 +56,20 @@ __global__ void __launch_bounds__(256) pbl_diag_kernel(const fpg_surface_cell* _
                                                        const fpg_surface_cell* __restrict__ s1, float alpha,
                                                        fpg_pbl_options o, uint32_t ncell, float* ustar_o,
                                                        float* wstar_o, float* hmix_o, float* oli_o, float* sshf_o,
-                                                       float* ssr_o, float* surfstr_o, float4* packed) {
+                                                       float* ssr_o, float* surfstr_o, float4* packed,
+                                                       CellHanna* hanna) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
-    pbl_cell(s0, s1, alpha, o, c, ustar_o, wstar_o, hmix_o, oli_o, sshf_o, ssr_o, surfstr_o, packed);
+    pbl_cell(s0, s1, alpha, o, c, ustar_o, wstar_o, hmix_o, oli_o, sshf_o, ssr_o, surfstr_o, packed, hanna);
 }
 
 __global__ void __launch_bounds__(256) pack_pbl_kernel(const float* __restrict__ u, const float* __restrict__ w,
                                                        const float* __restrict__ h, const float* __restrict__ o,
-                                                       uint32_t ncell, float4* packed) {
+                                                       uint32_t ncell, float4* packed, CellHanna* hanna) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < ncell) packed[c] = make_float4(u[c], w[c], h[c], o[c]);
+    if (c >= ncell) return;
+    packed[c] = make_float4(u[c], w[c], h[c], o[c]);
+    st_cell_hanna(hanna + c, cell_hanna(u[c], w[c], obukhov_from_inverse(o[c]), h[c]));
 }
 
 __global__ void __launch_bounds__(256) pack_frame_kernel(const float* __restrict__ u, const float* __restrict__ v,
@@ -197,9 +200,11 @@ extern "C" fpg_status fpg_pbl_create(fpg_ctx* ctx, size_t nx, size_t ny, fpg_pbl
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 7 && e == cudaSuccess; ++k) e = cudaMalloc(&p->field[k], n * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&p->packed, n * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc(&p->hanna, n * sizeof(CellHanna));
     if (e != cudaSuccess) {
         for (int k = 0; k < 7; ++k) cudaFree(p->field[k]);
         cudaFree(p->packed);
+        cudaFree(p->hanna);
         delete p;
         return cuda_status(e);
     }
@@ -211,6 +216,7 @@ extern "C" fpg_status fpg_pbl_destroy(fpg_pbl* p) {
     if (!p) return FPG_OK;
     for (int k = 0; k < 7; ++k) cudaFree(p->field[k]);
     cudaFree(p->packed);
+    cudaFree(p->hanna);
     delete p;
     return FPG_OK;
 }
@@ -227,7 +233,7 @@ extern "C" fpg_status fpg_pbl_upload(fpg_pbl* p, const float* ustar, const float
         else FPG_CUDA(cudaMemsetAsync(p->field[k], 0, n * sizeof(float), s));
     }
     pack_pbl_kernel<<<blocks_for(n, 256), 256, 0, s>>>(p->field[0], p->field[1], p->field[2], p->field[3],
-                                                        (uint32_t)n, p->packed);
+                                                        (uint32_t)n, p->packed, p->hanna);
     p->ctx->count();
     FPG_CHECK_LAUNCH();
     p->ready = true;
@@ -288,7 +294,8 @@ extern "C" fpg_status fpg_pbl_diagnostics(fpg_ctx* ctx, const fpg_surface* surfa
     const uint32_t n = (uint32_t)(pbl->nx * pbl->ny);
     pbl_diag_kernel<<<blocks_for(n, 256), 256, 0, s>>>(surface->frame[0], surface->frame[1], alpha, *options, n,
                                                         pbl->field[0], pbl->field[1], pbl->field[2], pbl->field[3],
-                                                        pbl->field[4], pbl->field[5], pbl->field[6], pbl->packed);
+                                                        pbl->field[4], pbl->field[5], pbl->field[6], pbl->packed,
+                                                        pbl->hanna);
     ctx->count();
     FPG_CHECK_LAUNCH();
     pbl->ready = true;
@@ -470,7 +477,7 @@ extern "C" fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* P, const fpg_met* me
         a.heights = met->heights_dev;
     }
     if (turb) {
-        a.pbl = pbl->packed;
+        a.hcell = pbl->hanna;
         a.pnx = (uint32_t)pbl->nx; a.pny = (uint32_t)pbl->ny;
         a.tdt = prm->turb_dt_seconds;
         a.rho = prm->rho_grad_over_rho;
@@ -599,12 +606,14 @@ __global__ void __launch_bounds__(256) langevin_record_kernel(RecordTurbArgs a) 
     hn.ust = r.ust; hn.wst = r.wst; hn.ol = r.ol; hn.h = r.h;
     hn.sigu = r.sigu; hn.sigv = r.sigv; hn.sigw = r.sigw; hn.dsigwdz = r.dsigwdz;
     hn.tlu = r.tlu; hn.tlv = r.tlv; hn.tlw = r.tlw;
-    // the branch hanna_short_w takes: its test on (L, max(h, 1))
-    hn.regime = hanna_regime(r.ol, fmaxf(r.h, 1.0f));
+    // the vertical re-evaluation's constants; its branch is hanna_short_w's
+    // test on (L, max(h, 1))
+    const CellHanna cell = cell_hanna(r.ust, r.wst, r.ol, r.h);
+    hn.regime = cell.regime;
     float pz = a.pos_z[p], tu = a.turb_u[p], tv = a.turb_v[p], tw = a.turb_w[p];
     const int32_t cbt_in = a.n_sub == 0u ? 0 : a.cbt[p];
     int32_t cbt = cbt_in;
-    turbulence_from_hanna<float, RecordLangevin>(a, hn, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
+    turbulence_from_hanna<float, RecordLangevin>(a, cell, hn, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
     a.turb_u[p] = tu; a.turb_v[p] = tv; a.turb_w[p] = tw;
     if (a.n_sub != 0u) {
         a.pos_z[p] = pz;

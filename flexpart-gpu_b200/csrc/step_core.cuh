@@ -26,8 +26,8 @@ struct StepArgs {
     uint32_t nx, ny, nz;
     int has_heights, monotonic;
     float alpha, dt, xs, ys, zs;
-    // turbulence
-    const float4* pbl;
+    // turbulence: the per-cell Hanna constants (pbl_cell)
+    const CellHanna* hcell;
     uint32_t pnx, pny;
     float tdt, rho, zmin;
     uint32_t n_sub;
@@ -180,8 +180,9 @@ struct RecordLangevin {
 // Jacobian: same values, bit for bit), the update policy and the argument
 // block (any type with tdt, rho, zmin and n_sub).
 template <class T, class L, class A>
-__device__ __forceinline__ void turbulence_from_hanna(const A& a, const HannaT<T>& hn, float2 e_uv, float2 e_w01,
-                                                      float2 e_w23, T& pz, T& tu, T& tv, T& tw, int32_t& cbt) {
+__device__ __forceinline__ void turbulence_from_hanna(const A& a, const CellHanna& cell, const HannaT<T>& hn,
+                                                      float2 e_uv, float2 e_w01, float2 e_w23, T& pz, T& tu, T& tv,
+                                                      T& tw, int32_t& cbt) {
     tu = L::h(tu, hn.sigu, hn.tlu, a.tdt, e_uv.x);
     tv = L::h(tv, hn.sigv, hn.tlv, a.tdt, e_uv.y);
     if (a.n_sub == 0u) {
@@ -205,7 +206,7 @@ __device__ __forceinline__ void turbulence_from_hanna(const A& a, const HannaT<T
             }
             pz = xclamp(z, zmin, h);
         }
-        if (sub < a.n_sub - 1u) hanna_short_w_t<T>(hn.ust, hn.wst, hn.ol, hn.h, pz, hn.regime, sigw, dsigwdz, tlw);
+        if (sub < a.n_sub - 1u) hanna_short_cell_t<T>(cell, pz, sigw, dsigwdz, tlw);
     }
 }
 
@@ -213,10 +214,11 @@ __device__ __forceinline__ void turbulence_from_hanna(const A& a, const HannaT<T
 // after the PBL lookup and the noise draws): Hanna at the particle height,
 // then turbulence_from_hanna.
 template <class T>
-__device__ __forceinline__ void turbulence_update(const StepArgs& a, float4 cell, float2 e_uv, float2 e_w01,
-                                                  float2 e_w23, T& pz, T& tu, T& tv, T& tw, int32_t& cbt) {
-    const HannaT<T> hn = compute_hanna_t<T>(cell.x, cell.y, obukhov_from_inverse(cell.w), cell.z, pz);
-    turbulence_from_hanna<T, HannaLangevin>(a, hn, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
+__device__ __forceinline__ void turbulence_update(const StepArgs& a, const CellHanna& cell, float2 e_uv,
+                                                  float2 e_w01, float2 e_w23, T& pz, T& tu, T& tv, T& tw,
+                                                  int32_t& cbt) {
+    const HannaT<T> hn = compute_hanna_cell_t<T>(cell, pz);
+    turbulence_from_hanna<T, HannaLangevin>(a, cell, hn, e_uv, e_w01, e_w23, pz, tu, tv, tw, cbt);
 }
 
 // What the step records for its adjoint (a policy of particle_step): NoTape
@@ -296,7 +298,7 @@ __device__ __forceinline__ void particle_step_t(const StepArgs& a, const float* 
         const float y = (float)cy + py;
         const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(a.pnx - 1u)));
         const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(a.pny - 1u)));
-        const float4 cell = __ldg(a.pbl + (i * a.pny + j));
+        const CellHanna cell = ld_cell_hanna(a.hcell + (i * a.pny + j));
 
         const uint32_t n_vert = a.n_sub > 1u ? a.n_sub : 1u;
         const uint32_t blocks = (2u + n_vert + 3u) / 4u;
@@ -394,7 +396,7 @@ __device__ __forceinline__ void pbl_cell(const fpg_surface_cell* __restrict__ s0
                                          const fpg_surface_cell* __restrict__ s1, float alpha,
                                          const fpg_pbl_options& o, uint32_t c, float* ustar_o, float* wstar_o,
                                          float* hmix_o, float* oli_o, float* sshf_o, float* ssr_o,
-                                         float* surfstr_o, float4* packed) {
+                                         float* surfstr_o, float4* packed, CellHanna* hanna) {
     float in[10];
     const float* a = &s0[c].surface_pressure_pa;
     const float* b = &s1[c].surface_pressure_pa;
@@ -466,6 +468,7 @@ __device__ __forceinline__ void pbl_cell(const fpg_surface_cell* __restrict__ s0
     ssr_o[c] = snn_(ssr, 0.0f);
     surfstr_o[c] = snn_(stress, 0.0f);
     packed[c] = make_float4(ustar, wstar, hmix, oli);
+    st_cell_hanna(hanna + c, cell_hanna(ustar, wstar, obukhov_from_inverse(oli), hmix));
 }
 
 __device__ __forceinline__ float snn0(float v) { return (finitef(v) && v > 0.0f) ? v : 0.0f; }
