@@ -166,9 +166,9 @@ __global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const 
                                                               const ScenDev* __restrict__ sc,
                                                               const uint2* __restrict__ items, uint32_t n_items,
                                                               uint32_t* work, TapeBase tb, uint32_t every) {
-    extern __shared__ float s_heights[];
+    extern __shared__ float s_levels[];
     __shared__ uint32_t s_item;
-    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
+    const Levels lv = stage_levels(a, s_levels);
     const float alpha = st->alpha;
     const uint32_t slice = st->step % tb.slices;
     TapeRec rec;
@@ -190,29 +190,20 @@ __global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const 
             reinterpret_cast<uint32_t*>(rec.t.f[T_FLAGS])[p] = 0u;
             continue;
         }
-        particle_step_t<TapeRec>(a, s_heights, p, local, alpha, d.counter, d.key0, d.key1, rec);
+        particle_step_t<TapeRec>(a, lv, p, local, alpha, d.counter, d.key0, d.key1, rec);
     }
 }
 
 // ---- reverse ----------------------------------------------------------------------
 
 // meters_to_level with its slope d(level)/dz.
-__device__ __forceinline__ float level_slope(const float* h, uint32_t nz, int has, int mono, float z) {
-    if (!has) return 1.0f;
+__device__ __forceinline__ float level_slope(const Levels& L, float z) {
+    if (!L.has) return 1.0f;
+    const float* h = L.h;
+    const uint32_t nz = L.nz;
     const float h0 = h[0];
     if (z <= h0) return h0 > 0.0f ? 1.0f / h0 : 0.0f;
-    uint32_t k;
-    if (mono) {
-        uint32_t lo = 1u, hi = nz;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (z <= h[mid]) hi = mid; else lo = mid + 1u;
-        }
-        k = lo;
-    } else {
-        k = nz;
-        for (uint32_t i = 1u; i < nz; ++i) if (z <= h[i]) { k = i; break; }
-    }
+    const uint32_t k = level_index(L, z);
     if (k >= nz) return 0.0f;
     const float denom = h[k] - h[k - 1u];
     return denom > 0.0f ? 1.0f / denom : 0.0f;
@@ -296,19 +287,19 @@ __device__ __forceinline__ void bias_add(const BiasTable& t, uint32_t n, float g
 // lanes with valid == false contribute nothing.  The bias terms of lanes
 // whose samples share a corner set are summed across the warp first, and
 // eight lanes then add one corner each to the CTA's table.
-__device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const float* hts, bool valid, float x, float y,
+__device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const Levels& lvl, bool valid, float x, float y,
                                              float z, float alpha, float lu, float lv, float lw,
                                              double* __restrict__ dbias, const BiasTable& table) {
     uint32_t x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
     axis_bracket(x, a.nx, x0, x1, tx);
     axis_bracket(y, a.ny, y0, y1, ty);
-    const float lev = meters_to_level(hts, a.nz, a.has_heights, a.monotonic, z);
+    const float lev = meters_to_level(lvl, z);
     axis_bracket(lev, a.nz, z0, z1, tz);
     const float ix = (x > 0.0f && x < (float)(a.nx - 1u)) ? 1.0f : 0.0f;
     const float iy = (y > 0.0f && y < (float)(a.ny - 1u)) ? 1.0f : 0.0f;
     const float iz = (lev > 0.0f && lev < (float)(a.nz - 1u))
-                         ? level_slope(hts, a.nz, a.has_heights, a.monotonic, z) : 0.0f;
+                         ? level_slope(lvl, z) : 0.0f;
     const uint32_t xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
     const float wx[2] = {1.0f - tx, tx}, wy[2] = {1.0f - ty, ty}, wz[2] = {1.0f - tz, tz};
     const float ta = 1.0f - alpha;
@@ -405,11 +396,11 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
                                                                  LamArrays lam, Receptors r,
                                                                  double* __restrict__ dbias,
                                                                  double* __restrict__ dsrc) {
-    extern __shared__ float s_heights[];
+    extern __shared__ float s_levels[];
     __shared__ uint32_t s_item;
     __shared__ uint32_t s_bias_key[kBiasTable];
     __shared__ float s_bias_g[3 * kBiasTable];
-    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
+    const Levels lvl = stage_levels(a, s_levels);
     for (uint32_t i = threadIdx.x; i < kBiasTable; i += blockDim.x) {
         s_bias_key[i] = kBiasEmpty;
         s_bias_g[3u * i] = 0.0f;
@@ -470,7 +461,7 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
         const float lu1 = lu0, lv1 = lv0, lw1 = lw0;
         ltu0 += lu1;
         ltv0 += lv1;
-        const float3 g1 = sample_vjp(a, s_heights, valid, px, py, pz, alpha, lu1, lv1, lw1, dbias, table);
+        const float3 g1 = sample_vjp(a, lvl, valid, px, py, pz, alpha, lu1, lv1, lw1, dbias, table);
         const float gpx = (fl & ADV_PX) ? g1.x : 0.0f;
         const float gpy = (fl & ADV_PY) ? g1.y : 0.0f;
         const float gpz = (fl & ADV_PZ) ? g1.z : 0.0f;
@@ -479,7 +470,7 @@ __global__ void __launch_bounds__(256, 4) inverse_adjoint_kernel(StepArgs a, con
         lz0 += gpz; lw0 += gpz * kz;
         ltu0 += lu0;
         ltv0 += lv0;
-        const float3 g0 = sample_vjp(a, s_heights, valid, x0, y0, z0, alpha, lu0, lv0, lw0, dbias, table);
+        const float3 g0 = sample_vjp(a, lvl, valid, x0, y0, z0, alpha, lu0, lv0, lw0, dbias, table);
         lx0 += g0.x; ly0 += g0.y; lz0 += g0.z;
         if (valid) {
             lam.f[L_X][p] = lx0; lam.f[L_Y][p] = ly0; lam.f[L_Z][p] = lz0;
@@ -623,7 +614,7 @@ static void enqueue_taped_step(fpg_inverse* v, bool sample, cudaStream_t s) {
     enqueue_pre(b, s);
     inverse_snapshot_kernel<<<1, 256, 0, s>>>(b->st, b->sc, (uint32_t)b->scen.size(), d.slices, d.st_all, d.sc_all);
     cudaMemsetAsync(d.work, 0, 4, s);
-    inverse_tape_kernel<<<d.grid_tape, 256, b->met->nz * sizeof(float), s>>>(make_step_args(b), b->st, b->sc,
+    inverse_tape_kernel<<<d.grid_tape, 256, level_smem_bytes(b->met), s>>>(make_step_args(b), b->st, b->sc,
                                                                              d.items, d.n_items, d.work,
                                                                              tape_base(v), d.cfg.sample_every_steps);
     b->ctx->count(2);
@@ -790,9 +781,11 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     int per_sm_tape = 0, per_sm_adj = 0;
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tape, inverse_tape_kernel, 256, nz * sizeof(float));
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tape, inverse_tape_kernel, 256,
+                                                          nz * sizeof(float) + FPG_LEVEL_BUCKETS);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adj, inverse_adjoint_kernel, 256, nz * sizeof(float));
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adj, inverse_adjoint_kernel, 256,
+                                                          nz * sizeof(float) + FPG_LEVEL_BUCKETS);
     if (e != cudaSuccess) {
         fpg_inverse_destroy(v);
         return cuda_status(e);
@@ -916,7 +909,7 @@ extern "C" fpg_status fpg_inverse_backward(fpg_inverse* v, const double* d_sim, 
     const Receptors rargs = d.receptors_args((uint32_t)b->met->nx, (uint32_t)b->met->ny);
     const LamArrays lam = lam_arrays(v);
     const TapeBase tb = tape_base(v);
-    const size_t smem = b->met->nz * sizeof(float);
+    const size_t smem = level_smem_bytes(b->met);
     const uint64_t n = b->total_steps;
     const uint32_t K = d.window, S = d.slices;
     const int64_t windows = d.n_windows;

@@ -140,9 +140,9 @@ template <int BLOCK, int MINB, int PPT>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_step_kernel(StepArgs a, BatchState* st,
                                                                  const ScenDev* __restrict__ sc,
                                                                  const uint2* __restrict__ items, uint32_t n_items) {
-    extern __shared__ float s_heights[];
+    extern __shared__ float s_levels[];
     __shared__ uint32_t s_item;
-    for (uint32_t i = threadIdx.x; i < a.nz; i += BLOCK) s_heights[i] = a.heights[i];
+    const Levels lv = stage_levels(a, s_levels);
     const float alpha = st->alpha;
     for (;;) {
         __syncthreads();
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_step_kernel(StepArgs a, Bat
         for (int j = 0; j < PPT; ++j) {
             const uint32_t local = w.y + (uint32_t)(j * BLOCK) + threadIdx.x;
             if (local < released)
-                particle_step(a, s_heights, d.offset + local, local, alpha, d.counter, d.key0, d.key1);
+                particle_step(a, lv, d.offset + local, local, alpha, d.counter, d.key0, d.key1);
         }
     }
 }
@@ -279,7 +279,9 @@ StepArgs make_step_args(fpg_batch* b) {
     a.heights = b->met->heights_dev;
     a.nx = (uint32_t)b->met->nx; a.ny = (uint32_t)b->met->ny; a.nz = (uint32_t)b->met->nz;
     a.has_heights = b->met->heights_set && b->met->heights[b->met->nz - 1] > 0.0f;
-    a.monotonic = b->met->monotonic;
+    a.level_mode = level_mode(b->met);
+    a.level_table = b->met->level_table_dev;
+    a.level_inv_w = b->met->level_inv_w;
     a.dt = (float)c.timestep_seconds;
     a.xs = c.x_grid_per_meter; a.ys = c.y_grid_per_meter; a.zs = c.z_grid_per_meter;
     a.hcell = b->pbl->hanna;
@@ -379,7 +381,7 @@ void enqueue_step_kernel(fpg_batch* b, cudaStream_t s) {
     const StepVariant& v = kVariants[b->variant];
     const StepArgs a = make_step_args(b);
     const uint32_t grid = (uint32_t)b->ctx->sm_count * std::max(b->resident[b->variant], 1u);
-    v.kernel<<<grid, v.block, b->met->nz * sizeof(float), s>>>(a, b->st, b->sc, b->items, b->n_items);
+    v.kernel<<<grid, v.block, level_smem_bytes(b->met), s>>>(a, b->st, b->sc, b->items, b->n_items);
     b->ctx->count(1);
 }
 
@@ -595,7 +597,7 @@ extern "C" fpg_status fpg_batch_create(fpg_ctx* ctx, const fpg_batch_config* cfg
     for (uint32_t v = 0; v < kNumVariants; ++v) {
         int per_sm = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].kernel, (int)kVariants[v].block,
-                                                          nz * sizeof(float));
+                                                          nz * sizeof(float) + FPG_LEVEL_BUCKETS);
         if (e != cudaSuccess) { fpg_batch_destroy(b); return cuda_status(e); }
         b->resident[v] = (uint32_t)std::max(per_sm, 1);
     }
@@ -698,7 +700,7 @@ extern "C" fpg_status fpg_batch_run_sequential(fpg_batch* b, uint32_t n_steps) {
             a.alpha = alpha;
             a.key0 = d.key0; a.key1 = d.key1;
             a.counter = counter;
-            fused_step_kernel<<<(released + 255) / 256, 256, b->met->nz * sizeof(float), s>>>(a);
+            fused_step_kernel<<<(released + 255) / 256, 256, level_smem_bytes(b->met), s>>>(a);
             b->ctx->count();
         }
         enqueue_post(b, s);

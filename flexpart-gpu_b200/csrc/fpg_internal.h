@@ -48,6 +48,10 @@ struct fpg_particles {
     int n_species = 1;
 };
 
+// Buckets of the metres->level table (one byte each, staged in shared
+// memory beside the level heights by every kernel that searches levels).
+constexpr uint32_t FPG_LEVEL_BUCKETS = 1024;
+
 struct fpg_met {
     fpg_ctx* ctx = nullptr;
     size_t nx = 0, ny = 0, nz = 0;
@@ -59,8 +63,18 @@ struct fpg_met {
     float heights[FPG_MAX_LEVELS] = {};
     bool heights_set = false;
     bool monotonic = true;
+    // Bucket table of the level search (heights non-decreasing with
+    // h[nz-1] > h[0]): bucket b of (z - h[0]) * level_inv_w holds the first
+    // level index, minus one, whose height is at least the lower edge of
+    // bucket b - 1, so the search scans up from there.
+    uint8_t* level_table_dev = nullptr;
+    float level_inv_w = 0.0f;
+    bool level_table = false;
     bool uploaded[2] = {false, false};
 };
+
+// Dynamic shared memory of a kernel that stages the level heights and table.
+inline size_t level_smem_bytes(const fpg_met* m) { return m->nz * sizeof(float) + FPG_LEVEL_BUCKETS; }
 
 struct fpg_pbl {
     fpg_ctx* ctx = nullptr;

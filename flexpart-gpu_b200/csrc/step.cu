@@ -20,9 +20,10 @@
 //   PBL: float4 (u*, w*, hmix, 1/L) per met cell, one 16-byte gather per
 //     particle;
 //   wet forcing per cell: float2 (lambda, fraction).
-// Level heights sit in shared memory; the metres->level search is a binary
-// search when heights are non-decreasing (same first index as the
-// reference's linear scan, advection_dual_wind.wgsl:94-117), else the scan.
+// Level heights sit in shared memory beside a 1024-bucket table of level
+// indices; for non-decreasing heights the metres->level search reads the
+// bucket's entry and scans up from it (same first index as the reference's
+// linear scan, advection_dual_wind.wgsl:94-117), else it runs the scan.
 //
 // The separated Hanna-record -> Langevin path (fpg_dispatch_hanna_params,
 // fpg_langevin_with_hanna) lives here too: it must give the fused kernel's
@@ -40,14 +41,15 @@
 namespace fpg {
 
 __global__ void __launch_bounds__(256, 5) fused_step_kernel(StepArgs a) {
-    extern __shared__ float s_heights[];
+    extern __shared__ float s_levels[];
+    Levels lv{};
     if (a.stages & FPG_STAGE_ADVECT) {
-        for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_heights[i] = a.heights[i];
+        lv = stage_levels(a, s_levels);
         __syncthreads();
     }
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
-    particle_step(a, s_heights, p, p, a.alpha, a.counter, a.key0, a.key1);
+    particle_step(a, lv, p, p, a.alpha, a.counter, a.key0, a.key1);
 }
 
 // ---- per-cell kernels --------------------------------------------------------
@@ -130,11 +132,13 @@ extern "C" fpg_status fpg_met_create(fpg_ctx* ctx, size_t nx, size_t ny, size_t 
     cudaError_t e = cudaMalloc(&m->bracket, nodes * 2 * sizeof(float4));
     if (e == cudaSuccess) e = cudaMalloc(&m->staging, nodes * 3 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&m->heights_dev, nz * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->level_table_dev, FPG_LEVEL_BUCKETS);
     if (e == cudaSuccess) e = cudaMemsetAsync(m->bracket, 0, nodes * 2 * sizeof(float4), ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(m->heights_dev, 0, nz * sizeof(float), ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
-        cudaFree(m->bracket); cudaFree(m->staging); cudaFree(m->heights_dev); delete m;
+        cudaFree(m->bracket); cudaFree(m->staging); cudaFree(m->heights_dev); cudaFree(m->level_table_dev);
+        delete m;
         return cuda_status(e);
     }
     *out = m;
@@ -146,6 +150,7 @@ extern "C" fpg_status fpg_met_destroy(fpg_met* m) {
     cudaFree(m->bracket);
     cudaFree(m->staging);
     cudaFree(m->heights_dev);
+    cudaFree(m->level_table_dev);
     delete m;
     return FPG_OK;
 }
@@ -181,11 +186,29 @@ extern "C" fpg_status fpg_met_set_level_heights(fpg_met* m, const float* heights
     if (n > FPG_MAX_LEVELS) return FPG_ERR_TOO_MANY_LEVELS;
     if (n != m->nz) return FPG_ERR_LENGTH_MISMATCH;
     std::memcpy(m->heights, heights, n * sizeof(float));
-    FPG_CUDA(cudaMemcpyAsync(m->heights_dev, m->heights, n * sizeof(float), cudaMemcpyHostToDevice, m->ctx->stream));
-    FPG_CUDA(cudaStreamSynchronize(m->ctx->stream));
     m->monotonic = true;
     for (size_t k = 1; k < n; ++k)
         if (!(heights[k] >= heights[k - 1])) m->monotonic = false;
+    // the bucket table of the level search: entry b is the first level (minus
+    // one) at or above the lower edge of bucket b - 1, in double, so that any
+    // z whose float bucket index is b lies above every level below it
+    uint8_t table[FPG_LEVEL_BUCKETS];
+    m->level_table = m->monotonic && n >= 2 && heights[n - 1] > heights[0] && std::isfinite(heights[0]) &&
+                     std::isfinite(heights[n - 1]);
+    if (m->level_table) {
+        const double h0 = heights[0], span = (double)heights[n - 1] - h0, w = span / FPG_LEVEL_BUCKETS;
+        m->level_inv_w = (float)(FPG_LEVEL_BUCKETS / span);
+        size_t k = 1;
+        for (uint32_t b = 0; b < FPG_LEVEL_BUCKETS; ++b) {
+            const double edge = h0 + ((double)b - 1.0) * w;
+            while (k < n && (double)heights[k] < edge) ++k;
+            table[b] = (uint8_t)(k - 1);
+        }
+        FPG_CUDA(cudaMemcpyAsync(m->level_table_dev, table, FPG_LEVEL_BUCKETS, cudaMemcpyHostToDevice,
+                                 m->ctx->stream));
+    }
+    FPG_CUDA(cudaMemcpyAsync(m->heights_dev, m->heights, n * sizeof(float), cudaMemcpyHostToDevice, m->ctx->stream));
+    FPG_CUDA(cudaStreamSynchronize(m->ctx->stream));
     m->heights_set = true;
     return FPG_OK;
 }
@@ -468,12 +491,14 @@ extern "C" fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* P, const fpg_met* me
         a.bracket = met->bracket;
         a.nx = (uint32_t)met->nx; a.ny = (uint32_t)met->ny; a.nz = (uint32_t)met->nz;
         a.has_heights = met->heights_set && met->heights[met->nz - 1] > 0.0f;
-        a.monotonic = met->monotonic;
+        a.level_mode = level_mode(met);
+        a.level_table = met->level_table_dev;
+        a.level_inv_w = met->level_inv_w;
         // gpu/advection.rs:639: alpha clamped to [0, 1]
         a.alpha = fminf(fmaxf(prm->alpha, 0.0f), 1.0f);
         a.dt = prm->dt_seconds;
         a.xs = prm->x_grid_per_meter; a.ys = prm->y_grid_per_meter; a.zs = prm->z_grid_per_meter;
-        smem = met->nz * sizeof(float);
+        smem = level_smem_bytes(met);
         a.heights = met->heights_dev;
     }
     if (turb) {

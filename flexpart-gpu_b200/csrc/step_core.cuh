@@ -23,8 +23,10 @@ struct StepArgs {
     // advection
     const float4* bracket;
     const float* heights;
+    const uint8_t* level_table;          // FPG_LEVEL_BUCKETS bytes when level_mode == LEVELS_TABLE
+    float level_inv_w;
     uint32_t nx, ny, nz;
-    int has_heights, monotonic;
+    int has_heights, level_mode;
     float alpha, dt, xs, ys, zs;
     // turbulence: the per-cell Hanna constants (pbl_cell)
     const CellHanna* hcell;
@@ -48,14 +50,50 @@ struct StepArgs {
     float* wet_prob;
 };
 
-// meters_to_grid_level (advection_dual_wind.wgsl:94-117).
-__device__ __forceinline__ float meters_to_level(const float* h, uint32_t nz, int has, int mono, float z) {
-    if (!has) return z;
-    const float h0 = h[0];
-    if (z <= h0) return h0 > 0.0f ? z / h0 : 0.0f;
+// How the level search runs: the reference's linear scan (heights not
+// sorted), a binary search (sorted), or a bucket table plus a short scan
+// (sorted with h[nz-1] > h[0]).  All three return the scan's index.
+enum { LEVELS_SCAN = 0, LEVELS_BISECT = 1, LEVELS_TABLE = 2 };
+
+// The search a met's heights allow (host side).
+inline int level_mode(const fpg_met* m) {
+    return m->level_table ? LEVELS_TABLE : m->monotonic ? LEVELS_BISECT : LEVELS_SCAN;
+}
+
+// The level heights and the bucket table as a kernel staged them in shared
+// memory (stage_levels).
+struct Levels {
+    const float* h;
+    const uint8_t* tab;
+    float inv_w;
+    uint32_t nz;
+    int has, mode;
+};
+
+// Copies the level heights (and the bucket table) into shared memory at
+// `smem` (level_smem_bytes of the met); the caller synchronises the block.
+__device__ __forceinline__ Levels stage_levels(const StepArgs& a, float* smem) {
+    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) smem[i] = a.heights[i];
+    uint32_t* tab = reinterpret_cast<uint32_t*>(smem + a.nz);
+    if (a.level_mode == LEVELS_TABLE)
+        for (uint32_t i = threadIdx.x; i < FPG_LEVEL_BUCKETS / 4u; i += blockDim.x)
+            tab[i] = __ldg(reinterpret_cast<const uint32_t*>(a.level_table) + i);
+    return Levels{smem, reinterpret_cast<const uint8_t*>(tab), a.level_inv_w, a.nz, a.has_heights, a.level_mode};
+}
+
+// The first k in [1, nz) with z <= h[k], nz if none (the loop of
+// advection_dual_wind.wgsl:101-110), for z > h[0].
+__device__ __forceinline__ uint32_t level_index(const Levels& L, float z) {
+    const float* h = L.h;
+    const uint32_t nz = L.nz;
     uint32_t k;
-    if (mono) {
-        // first k in [1, nz) with z <= h[k]; nz if none
+    if (L.mode == LEVELS_TABLE) {
+        // every level below the table's entry lies under z (the entry is
+        // taken one bucket low), so scanning up from it finds the same k
+        const uint32_t b = min(__float2uint_rz((z - h[0]) * L.inv_w), FPG_LEVEL_BUCKETS - 1u);
+        k = (uint32_t)L.tab[b] + 1u;
+        while (k < nz && !(z <= h[k])) ++k;
+    } else if (L.mode == LEVELS_BISECT) {
         uint32_t lo = 1u, hi = nz;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -66,6 +104,17 @@ __device__ __forceinline__ float meters_to_level(const float* h, uint32_t nz, in
         k = nz;
         for (uint32_t i = 1u; i < nz; ++i) if (z <= h[i]) { k = i; break; }
     }
+    return k;
+}
+
+// meters_to_grid_level (advection_dual_wind.wgsl:94-117).
+__device__ __forceinline__ float meters_to_level(const Levels& L, float z) {
+    if (!L.has) return z;
+    const float* h = L.h;
+    const uint32_t nz = L.nz;
+    const float h0 = h[0];
+    if (z <= h0) return h0 > 0.0f ? z / h0 : 0.0f;
+    const uint32_t k = level_index(L, z);
     if (k >= nz) return (float)(nz - 1u);
     const float hprev = h[k - 1u];
     const float denom = h[k] - hprev;
@@ -113,13 +162,13 @@ __device__ __forceinline__ Lerp6 lerp6(const Lerp6& a, const Lerp6& b, float t) 
                  lerpf(a.u1, b.u1, t), lerpf(a.v1, b.v1, t), lerpf(a.w1, b.w1, t)};
 }
 
-__device__ __forceinline__ float3 sample_dual(const StepArgs& a, const float* hts, float x, float y, float z,
+__device__ __forceinline__ float3 sample_dual(const StepArgs& a, const Levels& lv, float x, float y, float z,
                                               float alpha) {
     uint32_t x0, x1, y0, y1, z0, z1;
     float tx, ty, tz;
     axis_bracket(x, a.nx, x0, x1, tx);
     axis_bracket(y, a.ny, y0, y1, ty);
-    axis_bracket(meters_to_level(hts, a.nz, a.has_heights, a.monotonic, z), a.nz, z0, z1, tz);
+    axis_bracket(meters_to_level(lv, z), a.nz, z0, z1, tz);
     const uint32_t c00 = (x0 * a.ny + y0) * a.nz, c10 = (x1 * a.ny + y0) * a.nz;
     const uint32_t c01 = (x0 * a.ny + y1) * a.nz, c11 = (x1 * a.ny + y1) * a.nz;
     const float4* br = a.bracket;
@@ -240,7 +289,7 @@ __device__ __forceinline__ uint32_t inside(float v, float lo, float hi, uint32_t
 }
 
 template <class Tape>
-__device__ __forceinline__ void particle_step_t(const StepArgs& a, const float* s_heights, uint32_t p,
+__device__ __forceinline__ void particle_step_t(const StepArgs& a, const Levels& lv, uint32_t p,
                                                 uint32_t rng_index, float alpha, u32x4 counter, uint32_t key0,
                                                 uint32_t key1, Tape& tape) {
     const bool dry_on = (a.stages & FPG_STAGE_DRY) && a.dry_mode != FPG_FORCING_NONE;
@@ -260,17 +309,17 @@ __device__ __forceinline__ void particle_step_t(const StepArgs& a, const float* 
         const float x0 = (float)cx + px;
         const float y0 = (float)cy + py;
         const float z0 = pz;
-        const float3 s0 = sample_dual(a, s_heights, x0, y0, z0, alpha);
+        const float3 s0 = sample_dual(a, lv, x0, y0, z0, alpha);
         const float u0 = s0.x + tu, v0 = s0.y + tv, w0 = s0.z;
         const float xmax = (float)(a.nx - 1u), ymax = (float)(a.ny - 1u);
-        const float ztop = a.has_heights ? s_heights[a.nz - 1u] : (float)(a.nz - 1u);
+        const float ztop = a.has_heights ? lv.h[a.nz - 1u] : (float)(a.nz - 1u);
         const float rxp = x0 + (u0 * a.xs) * a.dt;
         const float ryp = y0 + (v0 * a.ys) * a.dt;
         const float rzp = z0 + (w0 * a.zs) * a.dt;
         const float pxp = clampf(rxp, 0.0f, xmax);
         const float pyp = clampf(ryp, 0.0f, ymax);
         const float pzp = clampf(rzp, 0.0f, ztop);
-        const float3 s1 = sample_dual(a, s_heights, pxp, pyp, pzp, alpha);
+        const float3 s1 = sample_dual(a, lv, pxp, pyp, pzp, alpha);
         const float u1 = s1.x + tu, v1 = s1.y + tv, w1 = s1.z;
         const float cu = 0.5f * (u0 + u1), cv = 0.5f * (v0 + v1), cw = 0.5f * (w0 + w1);
         const float rx1 = x0 + (cu * a.xs) * a.dt;
@@ -376,11 +425,11 @@ __device__ __forceinline__ void particle_step_t(const StepArgs& a, const float* 
     }
 }
 
-__device__ __forceinline__ void particle_step(const StepArgs& a, const float* s_heights, uint32_t p,
+__device__ __forceinline__ void particle_step(const StepArgs& a, const Levels& lv, uint32_t p,
                                               uint32_t rng_index, float alpha, u32x4 counter, uint32_t key0,
                                               uint32_t key1) {
     NoTape t;
-    particle_step_t<NoTape>(a, s_heights, p, rng_index, alpha, counter, key0, key1, t);
+    particle_step_t<NoTape>(a, lv, p, rng_index, alpha, counter, key0, key1, t);
 }
 
 

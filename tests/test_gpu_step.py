@@ -135,6 +135,37 @@ def test_legacy_level_index_mode_and_nonmonotonic_heights(ctx):
         _compare_state(p.download(), s, heights, rec, s64)
 
 
+@pytest.mark.parametrize("kind", ["stretched60", "duplicates", "two_levels"])
+def test_level_table_search_matches_the_scan(ctx, kind):
+    """The bucket-table level search (sorted heights) against the oracle's
+    linear scan (advection_dual_wind.wgsl:94-117): heights stretched to
+    15 km over 60 levels (several levels per bucket near the ground), heights
+    with repeated values, and two levels; particles exactly on level heights,
+    one ulp either side of them and of the bucket edges, and at random."""
+    if kind == "stretched60":
+        nz, hts = 60, (15000.0 * (np.arange(1, 61) / 60.0) ** 2).astype(np.float32)
+    elif kind == "duplicates":
+        hts = np.array([10, 10, 25, 25, 25, 60, 200, 200, 1000, 5000, 5000, 9000], np.float32)
+        nz = len(hts)
+    else:
+        nz, hts = 2, np.array([50.0, 3000.0], np.float32)
+    spec, frames, met = small_met(nz=nz)
+    met["heights"] = hts
+    rng = np.random.default_rng(nz)
+    edges = (hts[0] + (np.arange(1024) * (np.float64(hts[-1]) - hts[0]) / 1024.0)).astype(np.float32)[::7]
+    z = np.concatenate([hts, np.nextafter(hts, np.float32(np.inf)), np.nextafter(hts, np.float32(-np.inf)),
+                        edges, np.nextafter(edges, np.float32(0)),
+                        rng.uniform(0.0, 1.1 * float(hts[-1]), 2000).astype(np.float32)])
+    rec = population(spec.nx, spec.ny, len(z), seed=nz, inactive_every=0)
+    rec["pos_z"] = z
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.4, rec)
+    prm = production_params(alpha=0.4, stages=1)           # advection only
+    api.step(ctx, p, m, pbl, prm)
+    s = oracle_step(rec, met, None, prm)
+    s64 = oracle_step(rec, met, None, prm, np.float64)
+    _compare_state(p.download(), s, kind, rec, s64)
+
+
 def test_seam_functions_one_at_a_time(ctx):
     spec, frames, met = small_met(seed=4)
     rec = population(spec.nx, spec.ny, 1000, seed=21, z_max=60.0)
