@@ -38,7 +38,7 @@ namespace fpg {
 size_t particles_block_bytes(size_t capacity);
 
 // the plain fused step (step.cu), launched once per scenario by the sequential path
-__global__ void __launch_bounds__(256, 4) fused_step_kernel(StepArgs a);
+__global__ void __launch_bounds__(256, 5) fused_step_kernel(StepArgs a);
 
 namespace {
 

@@ -32,6 +32,7 @@ struct fpg_ctx {
     cudaStream_t stream = nullptr;
     int sm_count = 0;
     std::atomic<uint64_t> launches{0};
+    uint32_t step_shape = 0;                // launch shape of fpg_step (index into its compiled shapes)
     cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
     void count(uint64_t n = 1) { launches.fetch_add(n, std::memory_order_relaxed); }
 };

@@ -52,6 +52,42 @@ __global__ void __launch_bounds__(256, 5) fused_step_kernel(StepArgs a) {
     particle_step(a, lv, p, p, a.alpha, a.counter, a.key0, a.key1);
 }
 
+// The same pass under another launch shape: BLOCK threads per CTA compiled
+// for MINB resident CTAs per SM, PPT particles per thread (slots of one CTA
+// are contiguous; thread t takes t, t + BLOCK, ...).  Each particle's
+// arithmetic is the same, so the results are too.
+template <int BLOCK, int MINB, int PPT>
+__global__ void __launch_bounds__(BLOCK, MINB) fused_step_shape_kernel(StepArgs a) {
+    extern __shared__ float s_levels[];
+    Levels lv{};
+    if (a.stages & FPG_STAGE_ADVECT) {
+        lv = stage_levels(a, s_levels);
+        __syncthreads();
+    }
+    const size_t base = (size_t)blockIdx.x * (BLOCK * PPT) + threadIdx.x;
+#pragma unroll 1
+    for (int j = 0; j < PPT; ++j) {
+        const size_t p = base + (size_t)j * BLOCK;
+        if (p < a.n) particle_step(a, lv, (uint32_t)p, (uint32_t)p, a.alpha, a.counter, a.key0, a.key1);
+    }
+}
+
+struct StepShape {
+    uint32_t block, minb, ppt;
+    void (*kernel)(StepArgs);
+};
+
+// Shape 0 is fused_step_kernel itself (the default).
+const StepShape kStepShapes[] = {
+    {256, 5, 1, fused_step_kernel},
+    {256, 4, 1, fused_step_shape_kernel<256, 4, 1>},
+    {128, 10, 1, fused_step_shape_kernel<128, 10, 1>},
+    {256, 5, 2, fused_step_shape_kernel<256, 5, 2>},
+    {256, 5, 4, fused_step_shape_kernel<256, 5, 4>},
+    {512, 2, 1, fused_step_shape_kernel<512, 2, 1>},
+};
+constexpr uint32_t kNumStepShapes = sizeof(kStepShapes) / sizeof(kStepShapes[0]);
+
 // ---- per-cell kernels --------------------------------------------------------
 
 __global__ void __launch_bounds__(256) pbl_diag_kernel(const fpg_surface_cell* __restrict__ s0,
@@ -530,7 +566,8 @@ extern "C" fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* P, const fpg_met* me
     a.wet_prob = prm->wet_probability_dev;
 
     cudaStream_t s = ctx->pick(stream);
-    fused_step_kernel<<<blocks_for(n, 256), 256, smem, s>>>(a);
+    const StepShape& sh = kStepShapes[ctx->step_shape < kNumStepShapes ? ctx->step_shape : 0];
+    sh.kernel<<<blocks_for(n, sh.block * sh.ppt), sh.block, smem, s>>>(a);
     ctx->count();
     FPG_CHECK_LAUNCH();
     if (turb && next_counter) {
@@ -538,6 +575,91 @@ extern "C" fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* P, const fpg_met* me
         const uint64_t bpp = prm->n_substeps <= 2u ? 1u : 2u;
         counter_add64(prm->counter, (uint64_t)n * bpp, next_counter);
     }
+    return FPG_OK;
+}
+
+namespace fpg {
+size_t particles_block_bytes(size_t capacity);
+}
+
+extern "C" uint32_t fpg_step_tuning_candidates(fpg_batch_tuning* out, uint32_t max) {
+    for (uint32_t v = 0; out && v < kNumStepShapes && v < max; ++v)
+        out[v] = fpg_batch_tuning{kStepShapes[v].block, kStepShapes[v].minb, kStepShapes[v].ppt, 0.0f};
+    return kNumStepShapes;
+}
+
+extern "C" fpg_status fpg_step_set_tuning(fpg_ctx* ctx, const fpg_batch_tuning* t) {
+    if (!ctx || !t) return FPG_ERR_INVALID_ARGUMENT;
+    for (uint32_t v = 0; v < kNumStepShapes; ++v)
+        if (kStepShapes[v].block == t->block_threads && kStepShapes[v].minb == t->min_blocks_per_sm &&
+            kStepShapes[v].ppt == t->particles_per_thread) {
+            ctx->step_shape = v;
+            return FPG_OK;
+        }
+    return FPG_ERR_INVALID_ARGUMENT;
+}
+
+extern "C" fpg_status fpg_step_get_tuning(const fpg_ctx* ctx, fpg_batch_tuning* t) {
+    if (!ctx || !t) return FPG_ERR_INVALID_ARGUMENT;
+    const StepShape& sh = kStepShapes[ctx->step_shape < kNumStepShapes ? ctx->step_shape : 0];
+    *t = fpg_batch_tuning{sh.block, sh.minb, sh.ppt, 0.0f};
+    return FPG_OK;
+}
+
+// auto_tune_key_kernels (src/gpu/workgroup.rs:377-440) for the fused step:
+// every compiled shape timed from one snapshot of the particle arrays (the
+// restore copy also evicts them from L2), fastest kept.
+extern "C" fpg_status fpg_step_autotune(fpg_ctx* ctx, fpg_particles* P, const fpg_met* met, const fpg_pbl* pbl,
+                                        const fpg_step_params* prm, uint32_t reps, fpg_batch_tuning* results,
+                                        uint32_t max_results, fpg_batch_tuning* best, void* stream) {
+    if (!ctx || !P || !prm) return FPG_ERR_INVALID_ARGUMENT;
+    if (reps == 0) reps = 1;
+    cudaStream_t s = ctx->pick(stream);
+    const size_t bytes = particles_block_bytes(P->capacity);
+    const uint32_t keep = ctx->step_shape;
+    void* snap = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    fpg_status status = FPG_OK;
+    uint32_t best_v = keep < kNumStepShapes ? keep : 0;
+    float best_ms = 0.0f;
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMalloc(&snap, bytes);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(snap, P->block, bytes, cudaMemcpyDeviceToDevice, s);
+    for (uint32_t v = 0; e == cudaSuccess && status == FPG_OK && v < kNumStepShapes; ++v) {
+        ctx->step_shape = v;
+        float tmin = 0.0f;
+        for (uint32_t r = 0; r < reps; ++r) {
+            e = cudaMemcpyAsync(P->block, snap, bytes, cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+            if (e != cudaSuccess) break;
+            status = fpg_step(ctx, P, met, pbl, prm, nullptr, s);
+            if (status != FPG_OK) break;
+            e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) break;
+            if (r == 0 || ms < tmin) tmin = ms;
+        }
+        if (e != cudaSuccess || status != FPG_OK) break;
+        if (results && v < max_results)
+            results[v] = fpg_batch_tuning{kStepShapes[v].block, kStepShapes[v].minb, kStepShapes[v].ppt, tmin};
+        if (v == 0 || tmin < best_ms) { best_ms = tmin; best_v = v; }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(P->block, snap, bytes, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(snap);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess || status != FPG_OK) {
+        ctx->step_shape = keep;
+        return e != cudaSuccess ? cuda_status(e) : status;
+    }
+    ctx->step_shape = best_v;
+    if (best) *best = fpg_batch_tuning{kStepShapes[best_v].block, kStepShapes[best_v].minb, kStepShapes[best_v].ppt,
+                                       best_ms};
     return FPG_OK;
 }
 

@@ -90,6 +90,10 @@ _sig("fpg_cellfield_upload", _i32, _vp, _vp, _vp, _vp)
 _sig("fpg_cellfield_from_precipitation", _i32, _vp, _vp, _vp, _vp, _f32, _f32, _vp)
 _sig("fpg_step_params_default", None, ctypes.POINTER(StepParams))
 _sig("fpg_step", _i32, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams), _u32p, _vp)
+_sig("fpg_step_tuning_candidates", _u32, _vp, _u32)
+_sig("fpg_step_autotune", _i32, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams), _u32, _vp, _u32, _vp, _vp)
+_sig("fpg_step_set_tuning", _i32, _vp, _vp)
+_sig("fpg_step_get_tuning", _i32, _vp, _vp)
 _sig("fpg_advect_dual_wind", _i32, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _f32, _vp)
 _sig("fpg_langevin_fused", _i32, _vp, _vp, _vp, _f32, _f32, _u32, _f32, _u32p, _u32p, _u32p, _vp)
 _sig("fpg_dry_deposition", _i32, _vp, _vp, _vp, _f32, _f32, _vp, _vp)
@@ -186,6 +190,7 @@ EXPORTED = [
     "fpg_particles_create", "fpg_particles_destroy", "fpg_particles_capacity", "fpg_particles_dispatch_count",
     "fpg_particles_set_dispatch_count", "fpg_particles_upload", "fpg_particles_upload_slots",
     "fpg_particles_download", "fpg_particles_field", "fpg_particles_copy_field",
+    "fpg_step_tuning_candidates", "fpg_step_autotune", "fpg_step_set_tuning", "fpg_step_get_tuning",
     "fpg_met_create", "fpg_met_destroy", "fpg_met_upload_frame", "fpg_met_upload_frame_device",
     "fpg_met_set_level_heights",
     "fpg_pbl_create", "fpg_pbl_destroy", "fpg_pbl_upload", "fpg_pbl_download",

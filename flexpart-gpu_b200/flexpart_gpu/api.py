@@ -290,6 +290,48 @@ def step(ctx: Context, particles: Particles, met: Met | None, pbl: Pbl | None, p
     return list(nxt)
 
 
+def step_tuning_candidates() -> list[dict]:
+    """The compiled launch shapes of fpg_step."""
+    from .records import BatchTuning
+
+    n = lib.fpg_step_tuning_candidates(None, 0)
+    res = (BatchTuning * n)()
+    lib.fpg_step_tuning_candidates(res, n)
+    return [r.as_dict() for r in res]
+
+
+def step_autotune(ctx: Context, particles: Particles, met: Met | None, pbl: Pbl | None, params: StepParams,
+                  wet_cells: CellField | None = None, reps: int = 3, stream=None):
+    """fpg_step_autotune: times one step of `params` under every launch shape
+    (from a snapshot, restored afterwards; the counter does not advance) and
+    keeps the fastest in the context; returns (best, all candidates)."""
+    from .records import BatchTuning
+
+    if wet_cells is not None:
+        params.wet_cells = wet_cells.h.value
+    n = lib.fpg_step_tuning_candidates(None, 0)
+    res = (BatchTuning * n)()
+    best = BatchTuning()
+    check(lib.fpg_step_autotune(ctx.h, particles.h, met.h if met else None, pbl.h if pbl else None,
+                                ctypes.byref(params), reps, res, n, ctypes.byref(best), stream), "fpg_step_autotune")
+    return best.as_dict(), [r.as_dict() for r in res]
+
+
+def get_step_tuning(ctx: Context) -> dict:
+    from .records import BatchTuning
+
+    t = BatchTuning()
+    check(lib.fpg_step_get_tuning(ctx.h, ctypes.byref(t)), "fpg_step_get_tuning")
+    return t.as_dict()
+
+
+def set_step_tuning(ctx: Context, t: dict):
+    from .records import BatchTuning
+
+    bt = BatchTuning(t["block_threads"], t["min_blocks_per_sm"], t["particles_per_thread"], t.get("step_ms", 0.0))
+    check(lib.fpg_step_set_tuning(ctx.h, ctypes.byref(bt)), "fpg_step_set_tuning")
+
+
 def advect_dual_wind(ctx, particles, met, alpha, dt, xs=1.0, ys=1.0, zs=1.0):
     check(lib.fpg_advect_dual_wind(ctx.h, particles.h, met.h, alpha, dt, xs, ys, zs, None), "fpg_advect_dual_wind")
 

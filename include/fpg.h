@@ -326,6 +326,17 @@ typedef struct fpg_step_params {
  * min height 0.01 m, href 15 m, no deposition forcing, scales 1. */
 void fpg_step_params_default(fpg_step_params* params);
 
+/* A launch shape of a particle kernel: CUDA block size, resident blocks per
+ * SM the kernel is compiled for, particles per thread, and the time a tuner
+ * measured for it (0 when set by hand).  The batched step (fpg_driver.h)
+ * and the fused step share it. */
+typedef struct fpg_batch_tuning {
+    uint32_t block_threads;
+    uint32_t min_blocks_per_sm;
+    uint32_t particles_per_thread;
+    float step_ms;
+} fpg_batch_tuning;
+
 /* One fused pass over slots [0, dispatch_count) of `particles`, replacing, in
  * this order:
  *   encode_advection_dual_wind_gpu_with_kernel (src/gpu/advection.rs:605),
@@ -343,6 +354,27 @@ fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met,
                     uint32_t next_counter[4], void* stream);
 
 /* The four seam functions one at a time (same kernel, one stage). */
+/* Launch shapes of fpg_step: the counterpart of the reference's workgroup
+ * size autotune (auto_tune_key_kernels, src/gpu/workgroup.rs:377-440, which
+ * times each candidate workgroup size of the key kernels and keeps the
+ * fastest), over CUDA block size, resident blocks per SM and particles per
+ * thread.  Every shape gives the same results bit for bit.  The shape is a
+ * setting of the context (shape 0, <256, 5, 1>, until changed).
+ * fpg_step_tuning_candidates writes up to `max` compiled shapes and returns
+ * their count.  fpg_step_autotune times one fpg_step of `params` under every
+ * shape (best of `reps`), each from the same snapshot of the particle state,
+ * restores the state, keeps the fastest shape in the context and returns it
+ * in `best`; it needs device memory for one copy of the particle arrays, and
+ * the Philox counter is not advanced.  `results` (candidate order) and `best`
+ * may be NULL.  fpg_step_set_tuning selects a compiled shape
+ * (FPG_ERR_INVALID_ARGUMENT if none matches). */
+uint32_t fpg_step_tuning_candidates(fpg_batch_tuning* out, uint32_t max);
+fpg_status fpg_step_autotune(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met, const fpg_pbl* pbl,
+                             const fpg_step_params* params, uint32_t reps, fpg_batch_tuning* results,
+                             uint32_t max_results, fpg_batch_tuning* best, void* stream);
+fpg_status fpg_step_set_tuning(fpg_ctx* ctx, const fpg_batch_tuning* tuning);
+fpg_status fpg_step_get_tuning(const fpg_ctx* ctx, fpg_batch_tuning* tuning);
+
 fpg_status fpg_advect_dual_wind(fpg_ctx* ctx, fpg_particles* particles, const fpg_met* met,
                                 float alpha, float dt_seconds, float x_grid_per_meter,
                                 float y_grid_per_meter, float z_grid_per_meter, void* stream);

@@ -346,19 +346,13 @@ fpg_status fpg_batch_download_grids(fpg_batch* b, uint32_t* counts, uint32_t* ma
 /* Device-side error flags (1: a release fell outside the grid). */
 fpg_status fpg_batch_errors(fpg_batch* b, int32_t* flags);
 
-/* Launch shape of the persistent particle pass: threads per CTA, CTAs
- * resident per SM the kernel is compiled for (its register budget), and
- * particles per thread in one work item (a work item is block_threads *
- * particles_per_thread consecutive slots of one scenario).  step_ms is the
- * particle pass's time measured by the tuner (0 when set by hand). */
-typedef struct fpg_batch_tuning {
-    uint32_t block_threads;
-    uint32_t min_blocks_per_sm;
-    uint32_t particles_per_thread;
-    float step_ms;
-} fpg_batch_tuning;
-
-/* The compiled launch shapes: writes up to max of them, returns their count. */
+/* Launch shapes of the persistent particle pass (fpg_batch_tuning, fpg.h):
+ * threads per CTA, CTAs resident per SM the kernel is compiled for (its
+ * register budget), and particles per thread in one work item (a work item
+ * is block_threads * particles_per_thread consecutive slots of one
+ * scenario).  step_ms is the particle pass's time measured by the tuner (0
+ * when set by hand).
+ * The compiled launch shapes: writes up to max of them, returns their count. */
 uint32_t fpg_batch_tuning_candidates(fpg_batch_tuning* out, uint32_t max);
 /* Times the next step's particle pass under every compiled shape (best of
  * reps), each from the same snapshot of the live state, restores the state

@@ -110,6 +110,19 @@ def test_batch_tuning_candidates_listed_without_a_device():
     assert len(shapes) == len(c)
 
 
+def test_step_tuning_candidates_listed_without_a_device():
+    from flexpart_gpu import api
+    from flexpart_gpu import _lib
+
+    c = api.step_tuning_candidates()
+    shapes = [(t["block_threads"], t["min_blocks_per_sm"], t["particles_per_thread"]) for t in c]
+    assert shapes[0] == (256, 5, 1) and len(set(shapes)) == len(shapes) >= 4
+    lib = _lib.lib
+    assert lib.fpg_step_autotune(None, None, None, None, None, 1, None, 0, None, None) == -1
+    assert lib.fpg_step_set_tuning(None, None) == -1
+    assert lib.fpg_step_get_tuning(None, None) == -1
+
+
 def test_missing_library_fails_loudly(tmp_path):
     """No CPU fallback: without libfpg.so the package does not import."""
     import subprocess

@@ -166,6 +166,37 @@ def test_level_table_search_matches_the_scan(ctx, kind):
     _compare_state(p.download(), s, kind, rec, s64)
 
 
+def test_launch_shapes_give_the_same_bits_and_the_tuner_restores_the_state(ctx):
+    """Every compiled launch shape of fpg_step (block size, resident blocks,
+    particles per thread) gives the default shape's results bit for bit;
+    fpg_step_autotune leaves the particle state as it found it, keeps a
+    compiled shape, and the next step under it matches the default."""
+    spec, frames, met = small_met()
+    rec = population(spec.nx, spec.ny, 40_001, seed=3)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.6, rec)
+    prm = production_params(alpha=0.6, counter=(9, 0, 0, 0))
+    shapes = api.step_tuning_candidates()
+    out = []
+    for t in shapes:
+        api.set_step_tuning(ctx, t)
+        p.upload(rec)
+        api.step(ctx, p, m, pbl, prm)
+        out.append(p.download().tobytes())
+    assert all(o == out[0] for o in out[1:])
+    p.upload(rec)
+    best, cands = api.step_autotune(ctx, p, m, pbl, prm, reps=2)
+    assert p.download().tobytes() == rec.tobytes()             # state restored
+    key = (best["block_threads"], best["min_blocks_per_sm"], best["particles_per_thread"])
+    assert key in {(t["block_threads"], t["min_blocks_per_sm"], t["particles_per_thread"]) for t in shapes}
+    assert all(c["step_ms"] > 0.0 for c in cands) and best["step_ms"] == min(c["step_ms"] for c in cands)
+    got = api.get_step_tuning(ctx)
+    assert (got["block_threads"], got["min_blocks_per_sm"], got["particles_per_thread"]) == key
+    nxt = api.step(ctx, p, m, pbl, prm)
+    assert p.download().tobytes() == out[0]
+    assert nxt == orc.next_counter([9, 0, 0, 0], len(rec), 4)
+    api.set_step_tuning(ctx, shapes[0])
+
+
 def test_seam_functions_one_at_a_time(ctx):
     spec, frames, met = small_met(seed=4)
     rec = population(spec.nx, spec.ny, 1000, seed=21, z_max=60.0)
