@@ -912,6 +912,22 @@ def main():
         state["t"] = t + scn.dt
         state["k"] += 1
 
+    # launch shape of the step kernel: every compiled shape timed on the
+    # spun-up population from one snapshot (restored), the fastest kept
+    t0_ = state["t"]
+    fa_, fb_, ta_, tb_ = synthetic.bracket_frames(scn, t0_)
+    set_bracket(fa_, fb_)
+    state["bracket"] = (fa_, fb_, ta_)
+    alpha_ = (t0_ - ta_) / float(tb_ - ta_)
+    api.pbl_diagnostics(ctx, surf, alpha_, pbl)
+    tune_prm = StepParams.production(alpha=alpha_, dt_seconds=float(scn.dt), turb_dt_seconds=float(scn.dt),
+                                     x_grid_per_meter=xs, y_grid_per_meter=ys, z_grid_per_meter=zs, key=scn.key,
+                                     counter=state["counter"], dry_mode=1, dry_velocity_m_s=scn.dry_velocity,
+                                     wet_mode=3)
+    sorter.sort(parts, met)
+    step_best, step_cands = api.step_autotune(ctx, parts, met, pbl, tune_prm, wet_cells=wet, reps=3)
+    ctx.synchronize()
+
     for _ in range(args.warmup):
         one_step(False)
     ctx.synchronize()
@@ -1068,6 +1084,9 @@ def main():
                          # the bound that binds: warp-instruction issue (148 SMs x 4 per clock)
                          "issue": issue_roofline(n_active, avg_kernel_ms, clk)},
             "stages": stages,
+            "step_tuning": {"best": step_best, "candidates": step_cands,
+                            "how": "fpg_step_autotune on the spun-up, reordered population: each compiled shape "
+                                   "timed (best of 3) from one restored snapshot"},
             "clocks": clk,
             "gpu_launches": int(launches),
             "e2e": e2e,
