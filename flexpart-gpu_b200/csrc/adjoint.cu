@@ -72,6 +72,7 @@ struct Receptors {
     uint32_t every;
     const float* g;          // dL/dsim per receptor (backward)
     double* sim;             // forward sums
+    uint32_t* last_hit;      // per slot: 1 + the last step whose output state met a receptor cell (0: none)
 };
 
 struct Cic {
@@ -120,13 +121,20 @@ __global__ void __launch_bounds__(256) inverse_sample_kernel(const BatchState* s
         const float m = __uint_as_float(F.f[FPG_FIELD_MASS0][p]);
         const Cic c = cic(r, x, y, z);
         if (c.v == 0.0f) continue;
+        bool hit = false;
 #pragma unroll
         for (int di = 0; di < 2; ++di)
 #pragma unroll
             for (int dj = 0; dj < 2; ++dj) {
                 const int rr = receptor_at(r, d.instance, c.i0 + di, c.j0 + dj);
-                if (rr >= 0) atomicAdd(r.sim + rr, (double)(m * (c.wx[di] * c.wy[dj] * c.v)));
+                if (rr >= 0) {
+                    atomicAdd(r.sim + rr, (double)(m * (c.wx[di] * c.wy[dj] * c.v)));
+                    hit = true;
+                }
             }
+        // every receptor seed of this output state (receptor_seed) comes from
+        // these cells, whatever their weights
+        if (hit) r.last_hit[p] = st->step + 1u;
     }
 }
 
@@ -162,10 +170,15 @@ __global__ void inverse_snapshot_kernel(const BatchState* st, const ScenDev* __r
         sc_all[(size_t)j * n_scen + s] = sc[s];
 }
 
+// `live` (the recompute of a checkpoint window; NULL in the forward): a slot
+// whose last receptor hit came before this step has a zero adjoint from this
+// step on, so its tape is never read -- it is marked inactive for the
+// reverse and not stepped.
 __global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const BatchState* st,
                                                               const ScenDev* __restrict__ sc,
                                                               const uint2* __restrict__ items, uint32_t n_items,
-                                                              uint32_t* work, TapeBase tb, uint32_t every) {
+                                                              uint32_t* work, TapeBase tb, uint32_t every,
+                                                              const uint32_t* __restrict__ live) {
     extern __shared__ float s_levels[];
     __shared__ uint32_t s_item;
     const Levels lv = stage_levels(a, s_levels);
@@ -186,7 +199,7 @@ __global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const 
         const uint32_t local = w.y + threadIdx.x;
         if (local >= d.released) continue;
         const uint32_t p = d.offset + local;
-        if (!(a.flags[p] & FLAG_ACTIVE)) {
+        if (!(a.flags[p] & FLAG_ACTIVE) || (live && live[p] <= st->step)) {
             reinterpret_cast<uint32_t*>(rec.t.f[T_FLAGS])[p] = 0u;
             continue;
         }
@@ -533,6 +546,7 @@ struct InverseData {
     std::vector<fpg_receptor> receptors;
     int32_t* rmap = nullptr;
     double* sim = nullptr;
+    uint32_t* last_hit = nullptr;        // per slot, see Receptors
     float* g = nullptr;
     size_t nodes = 0;
     float4* ring_raw = nullptr;
@@ -577,6 +591,7 @@ struct InverseData {
         r.every = cfg.sample_every_steps;
         r.g = g;
         r.sim = sim;
+        r.last_hit = last_hit;
         return r;
     }
 };
@@ -608,6 +623,8 @@ static LamArrays lam_arrays(fpg_inverse* v) {
 
 // One taped step: the forward step with the tape pass in place of the plain
 // particle pass; `sample` adds the receptor sampling (forward runs).
+// The recompute (sample == false) steps only the slots whose adjoint is still
+// non-zero (live).
 static void enqueue_taped_step(fpg_inverse* v, bool sample, cudaStream_t s) {
     fpg_batch* b = v->b;
     InverseData& d = v->d;
@@ -616,7 +633,8 @@ static void enqueue_taped_step(fpg_inverse* v, bool sample, cudaStream_t s) {
     cudaMemsetAsync(d.work, 0, 4, s);
     inverse_tape_kernel<<<d.grid_tape, 256, level_smem_bytes(b->met), s>>>(make_step_args(b), b->st, b->sc,
                                                                              d.items, d.n_items, d.work,
-                                                                             tape_base(v), d.cfg.sample_every_steps);
+                                                                             tape_base(v), d.cfg.sample_every_steps,
+                                                                             sample ? nullptr : d.last_hit);
     b->ctx->count(2);
     if (sample) enqueue_inverse_sample(b, s);
     enqueue_end(b, s);
@@ -695,7 +713,7 @@ extern "C" fpg_status fpg_inverse_destroy(fpg_inverse* v) {
         if (d.tape_exec[k]) cudaGraphExecDestroy(d.tape_exec[k]);
         if (d.tape_graph[k]) cudaGraphDestroy(d.tape_graph[k]);
     }
-    cudaFree(d.rmap); cudaFree(d.sim); cudaFree(d.g); cudaFree(d.ring_raw); cudaFree(d.bias);
+    cudaFree(d.rmap); cudaFree(d.sim); cudaFree(d.last_hit); cudaFree(d.g); cudaFree(d.ring_raw); cudaFree(d.bias);
     cudaFree(d.ckpt); cudaFree(d.ckpt_st); cudaFree(d.ckpt_sc); cudaFree(d.st_all); cudaFree(d.sc_all);
     cudaFree(d.tape); cudaFree(d.lam); cudaFree(d.dbias); cudaFree(d.dbias_f); cudaFree(d.dsrc);
     cudaFree(d.items); cudaFree(d.work); cudaFree(d.work_rev);
@@ -755,6 +773,7 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     };
     cudaError_t e = alloc((void**)&d.rmap, rmap.size() * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.sim, std::max<size_t>(n_rec, 1) * 8);
+    if (e == cudaSuccess) e = alloc((void**)&d.last_hit, cap * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.g, std::max<size_t>(n_rec, 1) * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.ring_raw, d.nodes * bc.n_frames * sizeof(float4));
     if (e == cudaSuccess) e = alloc((void**)&d.bias, d.nodes * 3 * 4);
@@ -856,6 +875,7 @@ extern "C" fpg_status fpg_inverse_forward(fpg_inverse* v, double* simulated) {
     fpg_status st = batch_reset(b);
     if (st != FPG_OK) return st;
     FPG_CUDA(cudaMemsetAsync(d.sim, 0, std::max<size_t>(d.receptors.size(), 1) * 8, s));
+    FPG_CUDA(cudaMemsetAsync(d.last_hit, 0, v->b->capacity * 4, s));
     if (d.tape_in_forward) {
         if ((st = ensure_tape_graph(v, 1)) != FPG_OK) return st;
         for (uint64_t k = 0; k < b->total_steps; ++k) {
