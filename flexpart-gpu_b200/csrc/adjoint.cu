@@ -329,8 +329,8 @@ __device__ __forceinline__ float3 sample_vjp(const StepArgs& a, const Levels& lv
                 float fv = 0.0f;
                 if (act) {
                     const Node v = ld_node(a.bracket, (xs[i] * a.ny + ys[j]) * a.nz + zs[k]);
-                    fv = lu * (ta * v.u0 + alpha * v.u1) + lv * (ta * v.v0 + alpha * v.v1) +
-                         lw * (ta * v.w0 + alpha * v.w1);
+                    fv = lu * (ta * v.uv0.x + alpha * v.uv1.x) + lv * (ta * v.uv0.y + alpha * v.uv1.y) +
+                         lw * (ta * v.w01.x + alpha * v.w01.y);
                 }
                 f[i][j][k] = fv;
             }

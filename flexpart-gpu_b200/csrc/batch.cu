@@ -77,8 +77,7 @@ __global__ void __launch_bounds__(256) batch_pack_kernel(const BatchState* st, c
     const float4* f0 = ring + (size_t)st->fa * nodes;
     const float4* f1 = ring + (size_t)st->fb * nodes;
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < nodes; n += gridDim.x * blockDim.x) {
-        bracket[2u * n] = f0[n];
-        bracket[2u * n + 1u] = f1[n];
+        st_node(bracket, n, f0[n], f1[n]);
     }
 }
 
@@ -420,8 +419,7 @@ __global__ void __launch_bounds__(256) batch_pack_forced_kernel(const BatchState
     const float4* f0 = ring + (size_t)st->fa * nodes;
     const float4* f1 = ring + (size_t)st->fb * nodes;
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < nodes; n += gridDim.x * blockDim.x) {
-        bracket[2u * n] = f0[n];
-        bracket[2u * n + 1u] = f1[n];
+        st_node(bracket, n, f0[n], f1[n]);
     }
 }
 

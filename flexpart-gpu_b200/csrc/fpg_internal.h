@@ -56,8 +56,9 @@ constexpr uint32_t FPG_LEVEL_BUCKETS = 1024;
 struct fpg_met {
     fpg_ctx* ctx = nullptr;
     size_t nx = 0, ny = 0, nz = 0;
-    // Node-major bracket: node n holds float4 (u,v,w,0) of t0 at [2n] and of
-    // t1 at [2n+1]; node n = ((ix*ny)+iy)*nz+iz as in the reference layout.
+    // Node-major bracket: node n holds (u0, v0, u1, v1, w0, w1, 0, 0) of t0
+    // (0) and t1 (1) in bracket[2n], bracket[2n+1]; node n =
+    // ((ix*ny)+iy)*nz+iz as in the reference layout.
     float4* bracket = nullptr;
     float* staging = nullptr;               // 3*nodes floats for host uploads
     float* heights_dev = nullptr;           // nz level heights on the device

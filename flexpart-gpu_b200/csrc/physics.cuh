@@ -9,7 +9,8 @@
 // Transcendentals are CUDA's accurate expf/logf/exp2f/log2f/sincosf/cbrtf
 // (no fast-math intrinsics); sqrtf is correctly rounded, and '/' is too
 // except in the step's units (step.cu, batch.cu, adjoint.cu), which the
-// build compiles with the approximate full-range division (within 2 ulp).
+// build compiles with the approximate full-range division (within 2 ulp) and
+// with subnormal values flushed to zero.
 #pragma once
 
 #include <cstdint>

@@ -15,8 +15,9 @@
 // Data layout in HBM:
 //   particles: one 4-byte array per field, slot-indexed (coalesced 128-B
 //     warp accesses);
-//   wind bracket: node-major float4 pairs, t0 at [2n] and t1 at [2n+1]
-//     (u, v, w, 0) so the 8 corners of a sample cost 16 16-byte loads;
+//   wind bracket: node-major, 32 bytes per node (u0, v0, u1, v1, w0, w1,
+//     0, 0) of both frames, so the 8 corners of a sample cost 8 32-byte
+//     loads and the channels pair up for the packed FP32 lerps;
 //   PBL: float4 (u*, w*, hmix, 1/L) per met cell, one 16-byte gather per
 //     particle;
 //   wet forcing per cell: float2 (lambda, fraction).
@@ -114,7 +115,11 @@ __global__ void __launch_bounds__(256) pack_frame_kernel(const float* __restrict
                                                          const float* __restrict__ w, uint32_t nodes, int which,
                                                          float4* bracket) {
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < nodes) bracket[2u * n + (uint32_t)which] = make_float4(u[n], v[n], w[n], 0.0f);
+    // one frame's lanes of the node (u0, v0, u1, v1, w0, w1, 0, 0)
+    if (n >= nodes) return;
+    float* node = reinterpret_cast<float*>(bracket + 2u * n);
+    reinterpret_cast<float2*>(node)[which] = make_float2(u[n], v[n]);
+    node[4 + which] = w[n];
 }
 
 // wet_precipitation_state + below_cloud_scavenging_coefficient_gas

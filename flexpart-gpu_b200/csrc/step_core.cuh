@@ -133,33 +133,44 @@ __device__ __forceinline__ void axis_bracket(float coord, uint32_t n, uint32_t& 
 
 // sample_dual_{u,v,w} (advection_dual_wind.wgsl:142-236): trilinear in each
 // frame, then lerp by alpha.  The x-lerps of one (y, z) corner pair are taken
-// as soon as its four float4 (2 nodes x 2 frames) arrive, which keeps the
-// live registers at 16 floats instead of 64 while giving the same roundings
-// in the same order as the reference expression.
-struct Lerp6 { float u0, v0, w0, u1, v1, w1; };
+// as soon as its two nodes arrive, which keeps the live registers at 16
+// floats instead of 64 while giving the same roundings in the same order as
+// the reference expression.  The six channels (u, v, w of both frames) are
+// interpolated two at a time with the packed FP32 instructions of sm_100
+// (__fmul2_rn / __ffma2_rn: each lane is one IEEE round-to-nearest multiply
+// or fused multiply-add, so a lane's result is lerpf's bit for bit), on the
+// register pairs the node load fills: (u0, v0), (u1, v1), (w0, w1).
 
-// One bracket node (t0 u,v,w,0 | t1 u,v,w,0) is 32 bytes at a 32-byte
-// aligned offset (cudaMalloc base, node stride 32 B): one 256-bit load.
-struct Node { float u0, v0, w0, p0, u1, v1, w1, p1; };
+// One bracket node is 32 bytes at a 32-byte aligned offset (cudaMalloc base,
+// node stride 32 B), laid out (u0, v0, u1, v1, w0, w1, 0, 0) with frame 0
+// the bracket's t0: one 256-bit load, whose last two lanes are not used.
+struct Node { float2 uv0, uv1, w01; };
 
 __device__ __forceinline__ Node ld_node(const float4* br, uint32_t n) {
     Node v;
-    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-        : "=f"(v.u0), "=f"(v.v0), "=f"(v.w0), "=f"(v.p0), "=f"(v.u1), "=f"(v.v1), "=f"(v.w1), "=f"(v.p1)
+    asm("{\n.reg .f32 pad<2>;\nld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,pad0,pad1}, [%6];\n}"
+        : "=f"(v.uv0.x), "=f"(v.uv0.y), "=f"(v.uv1.x), "=f"(v.uv1.y), "=f"(v.w01.x), "=f"(v.w01.y)
         : "l"(br + 2u * n));
     return v;
 }
 
-__device__ __forceinline__ Lerp6 xpair(const float4* br, uint32_t na, uint32_t nb, float tx) {
-    const Node a = ld_node(br, na);
-    const Node b = ld_node(br, nb);
-    return Lerp6{lerpf(a.u0, b.u0, tx), lerpf(a.v0, b.v0, tx), lerpf(a.w0, b.w0, tx),
-                 lerpf(a.u1, b.u1, tx), lerpf(a.v1, b.v1, tx), lerpf(a.w1, b.w1, tx)};
+// The node layout from two frames' (u, v, w, 0).
+__device__ __forceinline__ void st_node(float4* br, uint32_t n, float4 f0, float4 f1) {
+    br[2u * n] = make_float4(f0.x, f0.y, f1.x, f1.y);
+    br[2u * n + 1u] = make_float4(f0.z, f1.z, 0.0f, 0.0f);
 }
 
-__device__ __forceinline__ Lerp6 lerp6(const Lerp6& a, const Lerp6& b, float t) {
-    return Lerp6{lerpf(a.u0, b.u0, t), lerpf(a.v0, b.v0, t), lerpf(a.w0, b.w0, t),
-                 lerpf(a.u1, b.u1, t), lerpf(a.v1, b.v1, t), lerpf(a.w1, b.w1, t)};
+// lerpf on two lanes: fmaf(a, 1 - t, b * t) with s = (1 - t, 1 - t).
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 s, float2 t) {
+    return __ffma2_rn(a, s, __fmul2_rn(b, t));
+}
+
+__device__ __forceinline__ Node lerp_node(const Node& a, const Node& b, float2 s, float2 t) {
+    return Node{lerp2(a.uv0, b.uv0, s, t), lerp2(a.uv1, b.uv1, s, t), lerp2(a.w01, b.w01, s, t)};
+}
+
+__device__ __forceinline__ Node xpair(const float4* br, uint32_t na, uint32_t nb, float2 s, float2 t) {
+    return lerp_node(ld_node(br, na), ld_node(br, nb), s, t);
 }
 
 __device__ __forceinline__ float3 sample_dual(const StepArgs& a, const Levels& lv, float x, float y, float z,
@@ -172,15 +183,20 @@ __device__ __forceinline__ float3 sample_dual(const StepArgs& a, const Levels& l
     const uint32_t c00 = (x0 * a.ny + y0) * a.nz, c10 = (x1 * a.ny + y0) * a.nz;
     const uint32_t c01 = (x0 * a.ny + y1) * a.nz, c11 = (x1 * a.ny + y1) * a.nz;
     const float4* br = a.bracket;
+    const float2 tx2 = make_float2(tx, tx), sx2 = make_float2(1.0f - tx, 1.0f - tx);
+    const float2 ty2 = make_float2(ty, ty), sy2 = make_float2(1.0f - ty, 1.0f - ty);
+    const float2 tz2 = make_float2(tz, tz), sz2 = make_float2(1.0f - tz, 1.0f - tz);
     // lerp(lerp(lerp(c000,c100,tx), lerp(c010,c110,tx), ty), lerp(lerp(c001,c101,tx), lerp(c011,c111,tx), ty), tz)
-    const Lerp6 l00 = xpair(br, c00 + z0, c10 + z0, tx);
-    const Lerp6 l10 = xpair(br, c01 + z0, c11 + z0, tx);
-    const Lerp6 l0 = lerp6(l00, l10, ty);
-    const Lerp6 l01 = xpair(br, c00 + z1, c10 + z1, tx);
-    const Lerp6 l11 = xpair(br, c01 + z1, c11 + z1, tx);
-    const Lerp6 l1 = lerp6(l01, l11, ty);
-    const Lerp6 t = lerp6(l0, l1, tz);
-    return make_float3(lerpf(t.u0, t.u1, alpha), lerpf(t.v0, t.v1, alpha), lerpf(t.w0, t.w1, alpha));
+    const Node l00 = xpair(br, c00 + z0, c10 + z0, sx2, tx2);
+    const Node l10 = xpair(br, c01 + z0, c11 + z0, sx2, tx2);
+    const Node l0 = lerp_node(l00, l10, sy2, ty2);
+    const Node l01 = xpair(br, c00 + z1, c10 + z1, sx2, tx2);
+    const Node l11 = xpair(br, c01 + z1, c11 + z1, sx2, tx2);
+    const Node l1 = lerp_node(l01, l11, sy2, ty2);
+    const Node t = lerp_node(l0, l1, sz2, tz2);
+    const float2 ta = make_float2(alpha, alpha), sa = make_float2(1.0f - alpha, 1.0f - alpha);
+    const float2 uv = lerp2(t.uv0, t.uv1, sa, ta);
+    return make_float3(uv.x, uv.y, lerpf(t.w01.x, t.w01.y, alpha));
 }
 
 // split_horizontal_coord (advection_dual_wind.wgsl:238-248).
