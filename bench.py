@@ -423,6 +423,9 @@ def run_batched(ctx, stream, args, rank, world):
     from flexpart_gpu import api, synthetic
     from flexpart_gpu import batch as bt
     from flexpart_gpu import timeloop as tl
+    import ctypes
+
+    lib = api._lib.lib
 
     ens = synthetic.config2(n_scenarios=args.batch_scenarios, seed=2 + rank)
     spec = ens.met
@@ -498,7 +501,12 @@ def run_batched(ctx, stream, args, rank, world):
     ms_e2e = timed(e2e)
     del b
 
-    # scenario-by-scenario plain driver runs over a subset
+    # scenario-by-scenario plain driver runs over a subset, every met frame
+    # and precipitation field resident on the device before the timed run
+    # (the driver's frame ring holds all of them; no host copy inside)
+    frame_dev = [{k: api.DeviceArray.from_numpy(ctx, f[k].reshape(-1)) for k in ("u", "v", "w")}
+                 | {"surface": api.DeviceArray.from_numpy(ctx, f["surface"].view(np.uint8))} for f in frames]
+    precip_dev = [api.DeviceArray.from_numpy(ctx, np.ascontiguousarray(p, np.float32)) for p in precs]
     sub = min(16, len(ens.sources))
     ps_sub = 0
     t_drv = 0.0
@@ -509,6 +517,11 @@ def run_batched(ctx, stream, args, rank, world):
         src = tl.BracketSource(scn, frames)
         cells = api.CellField(ctx, spec.nx, spec.ny)
         forcing = tl.cell_forcing(cells, dry_velocity=ens.dry_velocity)
+        drv.enable_met_ring(spec.n_frames)
+        for tf in range(scn.start, scn.end + spec.frame_seconds, spec.frame_seconds):
+            fd_ = frame_dev[((tf - scn.start) // spec.frame_seconds) % spec.n_frames]
+            drv.prefetch_frame(tf, *(fd_[k].ptr for k in ("u", "v", "w", "surface")))
+        ctx.synchronize()
 
         def run_one():
             last = None
@@ -516,7 +529,9 @@ def run_batched(ctx, stream, args, rank, world):
                 t = drv.current_time_seconds
                 fa = synthetic.bracket_frames(scn, t)[0]
                 if fa != last:
-                    cells.from_precipitation(precs[fa], a=ens.wet_a, b=ens.wet_b)
+                    api.check(lib.fpg_cellfield_from_precipitation(cells.h, ctypes.c_void_p(precip_dev[fa].ptr),
+                                                                   None, None, ens.wet_a, ens.wet_b, None),
+                              "wet cells")
                     last = fa
                 drv.run_timestep(src.at(t), forcing)
 
@@ -541,7 +556,10 @@ def run_batched(ctx, stream, args, rank, world):
                                            "per step, shared per-step kernels, no graph"},
         "per_scenario_driver": {"value": ps_sub / t_drv, "scenarios_timed": sub, "seconds": t_drv,
                                 "path": "fpg_forward_run_timestep per scenario, one plain run after another, "
-                                        "met from host"},
+                                        "every met frame resident in the driver's device frame ring"},
+        "speedup": ms_seq / ms,
+        "speedup_baseline": "sequential_interleaved: the same run as one plain fused-step launch per scenario "
+                            "per step (per-step kernels shared)",
         "speedup_vs_interleaved": ms_seq / ms,
         "speedup_vs_per_scenario_driver": value / world / (ps_sub / t_drv),
         "e2e": {"value": ps * world / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_run": h2d,
@@ -660,9 +678,14 @@ def run_adjoint(ctx, stream, args, rank, world):
                                        "device_bytes": bytes0},
             "taped_tail": {"tape_tail_windows": inv4.tape_tail_windows, "forward_ms": tf_t, "backward_ms": tb_t,
                            "ratio_to_forward": (tf_t + tb_t) / tf, "device_bytes": model.device_bytes},
-            "ratio_to_forward": (tf_t + tb_t) / tf,
-            "value": ps4 * world / ((tf_t + tb_t) / 1e3),
         }
+        # the headline is the faster mode: the recompute steps only the slots
+        # whose adjoint is non-zero, so with few slots reaching receptors it
+        # costs less than taping whole windows in the forward
+        best_ms = min(tf + tb, tf_t + tb_t)
+        out["c4"]["mode"] = "recompute_every_window" if tf + tb <= tf_t + tb_t else "taped_tail"
+        out["c4"]["ratio_to_forward"] = best_ms / tf
+        out["c4"]["value"] = ps4 * world / (best_ms / 1e3)
         del model
     return out
 

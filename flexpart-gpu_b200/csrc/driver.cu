@@ -650,10 +650,11 @@ extern "C" fpg_status fpg_forward_prefetch_frame(fpg_forward* d, int64_t t, cons
     const size_t nodes = d->met->nx * d->met->ny * d->met->nz, cells = d->met->nx * d->met->ny;
     cudaStream_t cs = d->copy_stream;
     FPG_CUDA(cudaStreamWaitEvent(cs, slot.released, 0));
-    FPG_CUDA(cudaMemcpyAsync(slot.uvw, u, nodes * sizeof(float), cudaMemcpyHostToDevice, cs));
-    FPG_CUDA(cudaMemcpyAsync(slot.uvw + nodes, v, nodes * sizeof(float), cudaMemcpyHostToDevice, cs));
-    FPG_CUDA(cudaMemcpyAsync(slot.uvw + 2 * nodes, w, nodes * sizeof(float), cudaMemcpyHostToDevice, cs));
-    FPG_CUDA(cudaMemcpyAsync(slot.surface, surface, cells * sizeof(fpg_surface_cell), cudaMemcpyHostToDevice, cs));
+    // host or device memory (the copy kind follows the pointer, unified addressing)
+    FPG_CUDA(cudaMemcpyAsync(slot.uvw, u, nodes * sizeof(float), cudaMemcpyDefault, cs));
+    FPG_CUDA(cudaMemcpyAsync(slot.uvw + nodes, v, nodes * sizeof(float), cudaMemcpyDefault, cs));
+    FPG_CUDA(cudaMemcpyAsync(slot.uvw + 2 * nodes, w, nodes * sizeof(float), cudaMemcpyDefault, cs));
+    FPG_CUDA(cudaMemcpyAsync(slot.surface, surface, cells * sizeof(fpg_surface_cell), cudaMemcpyDefault, cs));
     FPG_CUDA(cudaEventRecord(slot.copied, cs));
     slot.valid = true;
     slot.time = t;

@@ -43,20 +43,25 @@ __device__ __forceinline__ D2 operator*(const D2& x, const D2& y) {
 }
 __device__ __forceinline__ D2 operator*(const D2& x, float c) { return D2(x.v * c, x.a * c, x.b * c); }
 __device__ __forceinline__ D2 operator*(float c, const D2& x) { return D2(c * x.v, c * x.a, c * x.b); }
+// The value is the step's division (sdiv), as in the float code.
 __device__ __forceinline__ D2 operator/(const D2& x, const D2& y) {
-    const float q = x.v / y.v;
+    const float q = sdiv(x.v, y.v);
     const float r = __fdividef(1.0f, y.v);
     return D2(q, (x.a - q * y.a) * r, (x.b - q * y.b) * r);
 }
 __device__ __forceinline__ D2 operator/(const D2& x, float c) {
     const float r = __fdividef(1.0f, c);
-    return D2(x.v / c, x.a * r, x.b * r);
+    return D2(sdiv(x.v, c), x.a * r, x.b * r);
 }
 __device__ __forceinline__ D2 operator/(float c, const D2& y) {
-    const float q = c / y.v;
+    const float q = sdiv(c, y.v);
     const float r = -q * __fdividef(1.0f, y.v);
     return D2(q, r * y.a, r * y.b);
 }
+
+__device__ __forceinline__ D2 xdiv(const D2& x, const D2& y) { return x / y; }
+__device__ __forceinline__ D2 xdiv(const D2& x, float c) { return x / c; }
+__device__ __forceinline__ D2 xdiv(float c, const D2& y) { return c / y; }
 
 __device__ __forceinline__ D2 xexp(const D2& x) {
     const float e = expf(x.v);

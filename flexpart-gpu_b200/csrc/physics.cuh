@@ -25,6 +25,24 @@ __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(a, 1.0f - t, b * t); }
 __device__ __forceinline__ float sanitize_positive(float v) { return (finitef(v) && v > 0.0f) ? v : 0.0f; }
 
+// The division of the per-particle step.  The step's units are built with
+// FPG_RECIPROCAL_DIVISION: a / b is then a times the approximate reciprocal
+// of b (__fdividef), within 2 ulp for |b| in [2^-126, 2^126] -- the range
+// over which WGSL specifies x / y, to 2.5 ULP, for the reference's shaders --
+// and there the same bits as the approximate full-range division
+// (-prec-div=false; equal on 16.8 M random pairs with b in [1e-4, 1e5]) in
+// two instructions fewer.  The step divides by heights, velocity scales,
+// Lagrangian time scales and the Obukhov length, all inside that range.
+// Other units divide in IEEE arithmetic.
+__device__ __forceinline__ float sdiv(float a, float b) {
+#ifdef FPG_RECIPROCAL_DIVISION
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+__device__ __forceinline__ float xdiv(float a, float b) { return sdiv(a, b); }
+
 // x^(1/3), x^(2/3) and x^(-1/3) for x >= 0 from one cbrtf (max 1 ulp): the
 // reference writes pow(x, 1.0/3.0), pow(x, 2.0/3.0), pow(x, -1.0/3.0)
 // (hanna.rs:81-92, langevin_fused.wgsl:247-254,315-321).  The results stay
@@ -215,11 +233,11 @@ __device__ __forceinline__ void hanna_unstable_w(const CellHanna& c, T z, T zeta
     const T z23 = cz * cz;
     const T sigw_sq = c.k2 * (1.0f - 0.9f * zeta) * z23 + (1.8f - 1.4f * zeta) * c.ust * c.ust;
     sigw = xsqrt(sigw_sq) + 1.0e-2f;
-    const T zm13 = 1.0f / (val(zeta) >= 1.0e-3f ? cz : T(pow_third(1.0e-3f)));
-    dsigwdz = 0.5f / sigw / c.h * (c.k3 + c.k4 * (0.8f * zm13 - 1.8f * z23));
-    if (val(z) < fabsf(c.ol)) tlw = 0.1f * z / (sigw * (0.55f - 0.38f * xabs(z / c.ol)));
-    else if (val(zeta) < 0.1f) tlw = 0.59f * z / sigw;
-    else tlw = c.k5 / sigw * (1.0f - xexp(-5.0f * zeta));
+    const T zm13 = xdiv(1.0f, (val(zeta) >= 1.0e-3f ? cz : T(pow_third(1.0e-3f))));
+    dsigwdz = xdiv(xdiv(0.5f, sigw), c.h) * (c.k3 + c.k4 * (0.8f * zm13 - 1.8f * z23));
+    if (val(z) < fabsf(c.ol)) tlw = xdiv(0.1f * z, sigw * (0.55f - 0.38f * xabs(xdiv(z, c.ol))));
+    else if (val(zeta) < 0.1f) tlw = xdiv(0.59f * z, sigw);
+    else tlw = xdiv(c.k5, sigw) * (1.0f - xexp(-5.0f * zeta));
 }
 
 // compute_hanna_params (physics/hanna.rs:49-163) at height z_in of a cell.
@@ -228,17 +246,17 @@ __device__ __forceinline__ HannaT<T> compute_hanna_cell_t(const CellHanna& c, T 
     HannaT<T> o;
     const float ust = c.ust, h = c.h;
     const T z = xclamp(z_in, 0.0f, h);
-    const T zeta = xclamp(z / h, 0.0f, 1.0f);
+    const T zeta = xclamp(xdiv(z, h), 0.0f, 1.0f);
     T sigu, sigv, sigw, dsigwdz, tlu, tlv, tlw;
     o.regime = c.regime;
     if (c.regime == REGIME_NEUTRAL) {
-        const T corr = z / ust;
+        const T corr = xdiv(z, ust);
         sigu = 1.0e-2f + c.k0 * xexp(-3.0e-4f * corr);
         sigw = c.k1 * xexp(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
         sigv = sigw;
-        tlu = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
+        tlu = xdiv(xdiv(0.5f * z, sigw), (1.0f + 1.5e-3f * corr));
         tlv = tlu;
         tlw = tlu;
         tlu = xmax(tlu, 10.0f);
@@ -269,9 +287,9 @@ __device__ __forceinline__ HannaT<T> compute_hanna_cell_t(const CellHanna& c, T 
         sigv = 1.0e-2f + c.k1 * (1.0f - zeta);
         sigw = sigv;
         dsigwdz = T(c.k2);                       // the cell's, already final
-        tlu = c.k5 / sigu * xsqrt(zeta);
+        tlu = xdiv(c.k5, sigu) * xsqrt(zeta);
         tlv = 0.467f * tlu;
-        tlw = c.k6 / sigw * xpow(zeta, 0.8f);
+        tlw = xdiv(c.k6, sigw) * xpow(zeta, 0.8f);
         tlu = xmax(tlu, 10.0f);
         tlv = xmax(tlv, 10.0f);
         tlw = xmax(tlw, 30.0f);
@@ -304,20 +322,20 @@ __device__ __forceinline__ Hanna compute_hanna(float ust_in, float wst_in, float
 template <class T>
 __device__ __forceinline__ void hanna_short_cell_t(const CellHanna& c, T z_in, T& sigw_o, T& dsigwdz_o, T& tlw_o) {
     const T z = xclamp(z_in, 0.0f, c.h);
-    const T zeta = xclamp(z / c.h, 0.0f, 1.0f);
+    const T zeta = xclamp(xdiv(z, c.h), 0.0f, 1.0f);
     T sigw, dsigwdz, tlw;
     if (c.regime == REGIME_NEUTRAL) {
-        const T corr = z / c.ust;
+        const T corr = xdiv(z, c.ust);
         sigw = c.k1 * xexp(-2.0e-4f * corr);
         dsigwdz = -2.0e-4f * sigw;
         sigw = sigw + 1.0e-2f;
-        tlw = 0.5f * z / sigw / (1.0f + 1.5e-3f * corr);
+        tlw = xdiv(xdiv(0.5f * z, sigw), (1.0f + 1.5e-3f * corr));
     } else if (c.regime == REGIME_UNSTABLE) {
         hanna_unstable_w<T>(c, z, zeta, sigw, dsigwdz, tlw);
     } else {
         sigw = 1.0e-2f + c.k1 * (1.0f - zeta);
         dsigwdz = T(c.k2);                       // the cell's, already final
-        tlw = c.k6 / sigw * xpow(zeta, 0.8f);
+        tlw = xdiv(c.k6, sigw) * xpow(zeta, 0.8f);
     }
     tlw = xmax(tlw, 30.0f);
     if (c.regime != REGIME_STABLE) {
@@ -350,7 +368,7 @@ __device__ __forceinline__ void hanna_short_w(float ust_in, float wst_in, float 
 // ---- Langevin OU updates (physics/langevin.rs:116-170, langevin_fused.wgsl:350-389)
 template <class T>
 __device__ __forceinline__ T langevin_h_t(T prev, T sigma, T tl, float dt, float eta) {
-    const T ratio = dt / tl;
+    const T ratio = xdiv(dt, tl);
     T next;
     if (val(ratio) < 0.5f) {
         next = (1.0f - ratio) * prev + eta * sigma * xsqrt(xmax(2.0f * ratio, 0.0f));
@@ -364,7 +382,7 @@ __device__ __forceinline__ T langevin_h_t(T prev, T sigma, T tl, float dt, float
 template <class T>
 __device__ __forceinline__ T langevin_v_t(T prev, T sigma_w, T tlw, T dsigwdz, float dt, float rho, float eta) {
     const T drift = sigma_w * (dsigwdz + rho * sigma_w);
-    const T ratio = dt / tlw;
+    const T ratio = xdiv(dt, tlw);
     T next;
     if (val(ratio) < 0.5f) {
         next = (1.0f - ratio) * prev + eta * sigma_w * xsqrt(xmax(2.0f * ratio, 0.0f)) + dt * drift;
@@ -387,7 +405,7 @@ __device__ __forceinline__ float langevin_v(float prev, float sigma_w, float tlw
 // ---- Deposition --------------------------------------------------------------
 // dry_deposition.wgsl:70-74 (survival factor; href already floored at 0.1 m).
 __device__ __forceinline__ float dry_survival(float vdep, float dt, float href) {
-    const float exponent = -fmaxf(vdep, 0.0f) * fabsf(dt) / (2.0f * href);
+    const float exponent = sdiv(-fmaxf(vdep, 0.0f) * fabsf(dt), 2.0f * href);
     return clampf(expf(exponent), 0.0f, 1.0f);
 }
 

@@ -113,12 +113,12 @@ __device__ __forceinline__ float meters_to_level(const Levels& L, float z) {
     const float* h = L.h;
     const uint32_t nz = L.nz;
     const float h0 = h[0];
-    if (z <= h0) return h0 > 0.0f ? z / h0 : 0.0f;
+    if (z <= h0) return h0 > 0.0f ? sdiv(z, h0) : 0.0f;
     const uint32_t k = level_index(L, z);
     if (k >= nz) return (float)(nz - 1u);
     const float hprev = h[k - 1u];
     const float denom = h[k] - hprev;
-    if (denom > 0.0f) return (float)(k - 1u) + (z - hprev) / denom;
+    if (denom > 0.0f) return (float)(k - 1u) + sdiv(z - hprev, denom);
     return (float)(k - 1u);
 }
 
@@ -254,7 +254,7 @@ __device__ __forceinline__ void turbulence_from_hanna(const A& a, const CellHann
         tw = L::v(tw, hn.sigw, hn.tlw, hn.dsigwdz, a.tdt, a.rho, e_w01.x);
         return;
     }
-    const float dt_sub = a.tdt / (float)a.n_sub;
+    const float dt_sub = sdiv(a.tdt, (float)a.n_sub);
     const float h = hn.h;
     const float zmin = a.zmin;
     T sigw = hn.sigw, dsigwdz = hn.dsigwdz, tlw = hn.tlw;

@@ -137,8 +137,9 @@ fpg_status fpg_forward_accumulate_grid(fpg_forward* d, fpg_grid* grid, uint32_t 
  * frames (u, v, w and surface cells) on the device, filled ahead of use on a
  * separate copy stream.  fpg_forward_prefetch_frame queues the copy of the
  * frame valid at time_seconds and returns without waiting (page-locked host
- * buffers, fpg_host_alloc, make the copy overlap the steps; the host
- * buffers must stay unchanged until the frame is used).  When run_timestep
+ * buffers, fpg_host_alloc, make the copy overlap the steps; device buffers
+ * are copied on the device; either must stay unchanged until the frame is
+ * used).  When run_timestep
  * meets a new bracket whose two frames are in the ring, it repacks them on
  * the device after their copies (no host copy, the bracket's host pointers
  * are not read); otherwise it uploads from the bracket's host pointers as

@@ -144,24 +144,33 @@ def _run_with_ring(ctx, scn, frames, mode):
     if mode != "host":
         drv.enable_met_ring(3)
     prefetched = set()
+    dev = None
+    if mode == "device":
+        # the frames resident on the device: the ring copies device to device
+        dev = [{k: api.DeviceArray.from_numpy(ctx, np.ascontiguousarray(f[k]).view(np.uint8))
+                for k in ("u", "v", "w", "surface")} for f in src.frames]
 
     def prefetch(tf):
         if tf not in prefetched:
-            f = src.frames[((tf - scn.start) // fs) % scn.met.n_frames]
-            drv.prefetch_frame(tf, f["u"], f["v"], f["w"], f["surface"])
+            k = ((tf - scn.start) // fs) % scn.met.n_frames
+            if dev is None:
+                f = src.frames[k]
+                drv.prefetch_frame(tf, f["u"], f["v"], f["w"], f["surface"])
+            else:
+                drv.prefetch_frame(tf, *(dev[k][c].ptr for c in ("u", "v", "w", "surface")))
             prefetched.add(tf)
 
     while drv.has_remaining_steps:
         t = drv.current_time_seconds
         _, _, ta, tb = synthetic.bracket_frames(scn, t)
-        if mode == "ring" and t == scn.start:
+        if mode in ("ring", "device") and t == scn.start:
             prefetch(ta)
             prefetch(tb)
         if mode == "mixed" and ((ta - scn.start) // fs) % 2 == 0:
             prefetch(ta)
             prefetch(tb)
         drv.run_timestep(src.at(t), forcing)
-        if mode == "ring":
+        if mode in ("ring", "device"):
             prefetch(tb + fs)      # the next bracket's new frame, once this bracket is in use
     drv.finalize()
     return drv.particles.download(), drv.met_ring_stats()
@@ -173,11 +182,13 @@ def test_met_ring_streaming_gives_identical_results(ctx):
     host, (h0, u0) = _run_with_ring(ctx, scn, frames, "host")
     ring, (h1, u1) = _run_with_ring(ctx, scn, frames, "ring")
     mixed, (h2, u2) = _run_with_ring(ctx, scn, frames, "mixed")
+    device, (h3, u3) = _run_with_ring(ctx, scn, frames, "device")
     brackets = 8          # 24 h of 3 h brackets
     assert (h0, u0) == (0, brackets)
     assert (h1, u1) == (brackets, 0)
     assert (h2, u2) == (brackets // 2, brackets // 2)
-    assert host.tobytes() == ring.tobytes() == mixed.tobytes()
+    assert (h3, u3) == (brackets, 0)
+    assert host.tobytes() == ring.tobytes() == mixed.tobytes() == device.tobytes()
 
 
 def test_device_grid_written_as_netcdf_snapshot(ctx, tmp_path):
