@@ -63,14 +63,16 @@ ADJOINT_HBM_BUDGET = 140e9  # device bytes the batched adjoint may hold (the 150
 # the order decays; a reorder costs 0.92 ms).  The default window of timed
 # steps is one reorder period, and its first step reorders.
 SORT_EVERY = 96
-# DRAM bytes (read + write) per particle of one fused_step_kernel launch, from
-# an ncu capture of a 2 M-particle launch (131.1 MB), scaled by the particle
-# count; below the algorithmic 96 B because part of the state was still in
-# the 126 MB L2 across the capture's replay passes.
-DRAM_BYTES_PER_PARTICLE_NCU = 131.1e6 / 2.0e6
-# Warp instructions per 32 particle-steps of fused_step_kernel
-# (smsp__inst_executed.sum of the same capture: 158.3 M for 2 M particles).
-WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 158.3e6 / (2.0e6 / 32)
+# DRAM bytes (read + write) per particle of one fused-step launch, from an
+# ncu capture of a 10 M-particle launch of the global run's population
+# (bench.py --quick: particles around the 8 sources, reordered by met cell
+# before the timed steps): 443.3 MB read + 423.3 MB written = 86.7 B per
+# particle against the algorithmic 96 B (44 B read, 52 B written); the last
+# ~100 MB of writes are still in the 126 MB L2 when the kernel ends.
+DRAM_BYTES_PER_PARTICLE_NCU = (443.3e6 + 423.3e6) / 10.0e6
+# Warp instructions per 32 particle-steps (smsp__inst_executed.sum of the
+# same capture: 641.5 M for 10 M particles).
+WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 641.5e6 / (10.0e6 / 32)
 
 
 def issue_roofline(n_particles, kernel_ms, clk):
@@ -87,7 +89,7 @@ def issue_roofline(n_particles, kernel_ms, clk):
     peak = sms * 4 * mhz * 1e6
     return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
             "instructions_per_launch": instr, "sm_mhz": mhz,
-            "source": "smsp__inst_executed.sum of a 2M-particle ncu capture, scaled by particles"}
+            "source": "smsp__inst_executed.sum of a 10M-particle ncu capture (bench.py --quick), scaled by particles"}
 
 
 def parse():
@@ -1100,7 +1102,8 @@ def main():
                        "l2": "inputs larger than L2 (960 MB particle state per step)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE_NCU * n_active,
-                         "traffic_source": "ncu dram__bytes_read+write of a 2M-particle launch, scaled by particles",
+                         "traffic_source": "ncu dram__bytes_read+write of a 10M-particle launch (bench.py --quick), "
+                                           "scaled by particles",
                          "peak_kind": peak_kind,
                          "kernel": "fused_step_kernel", "kernel_ms": avg_kernel_ms,
                          "bytes_per_launch": BYTES_PER_PARTICLE_STEP * n_active,
