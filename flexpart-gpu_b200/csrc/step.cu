@@ -86,6 +86,8 @@ const StepShape kStepShapes[] = {
     {256, 5, 2, fused_step_shape_kernel<256, 5, 2>},
     {256, 5, 4, fused_step_shape_kernel<256, 5, 4>},
     {512, 2, 1, fused_step_shape_kernel<512, 2, 1>},
+    {256, 6, 1, fused_step_shape_kernel<256, 6, 1>},
+    {128, 12, 1, fused_step_shape_kernel<128, 12, 1>},
 };
 constexpr uint32_t kNumStepShapes = sizeof(kStepShapes) / sizeof(kStepShapes[0]);
 
