@@ -64,7 +64,7 @@ __device__ __forceinline__ D2 xdiv(const D2& x, float c) { return x / c; }
 __device__ __forceinline__ D2 xdiv(float c, const D2& y) { return c / y; }
 
 __device__ __forceinline__ D2 xexp(const D2& x) {
-    const float e = expf(x.v);
+    const float e = xexp(x.v);
     return D2(e, e * x.a, e * x.b);
 }
 __device__ __forceinline__ D2 xsqrt(const D2& x) {

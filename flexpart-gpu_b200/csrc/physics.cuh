@@ -101,16 +101,23 @@ __device__ __forceinline__ float2 box_muller(float u0, float u1) {
 // which carries derivatives beside the value and supplies the same helper
 // names.  For float every helper is the plain CUDA call, so the float
 // instantiation performs exactly the operations written, in the same order.
+//
+// The exponentials and powers of the Hanna profiles and the Langevin updates
+// run at the accuracy WGSL specifies for the reference's shaders, which
+// compute them (langevin_fused.wgsl:224-389): exp within 3 + 2|x| ulp, pow
+// inherited from exp2(y log2 x).  CUDA's __expf stays within 2 +
+// floor(1.173|x|) ulp and __powf is exp2 of y times the hardware log2, the
+// same construction as WGSL's pow; both cost a few instructions where expf
+// and powf cost 9 and about 30, and a particle-step takes up to seven
+// exponentials and four powers.
 __device__ __forceinline__ float val(float x) { return x; }
-__device__ __forceinline__ float xexp(float x) { return expf(x); }
+__device__ __forceinline__ float xexp(float x) { return __expf(x); }
 __device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ float xcbrt(float x) { return pow_third(x); }
-// x^e for x > 0 as 2^(e log2 x) from CUDA's exp2f and log2f: the reference's
-// pow(zeta, 0.8) of the stable-branch T_L (hanna.rs:111,
-// langevin_fused.wgsl:271,332) within a few ulp of powf, at a
-// fraction of its cost (the stable branch runs up to four times per
-// particle-step).  x <= 0 goes to powf (0^0.8 = 0).
-__device__ __forceinline__ float pow_pos(float x, float e) { return x > 0.0f ? exp2f(e * log2f(x)) : powf(x, e); }
+// x^e for x > 0 by __powf: the reference's pow(zeta, 0.8) of the
+// stable-branch T_L (hanna.rs:111, langevin_fused.wgsl:271,332).  x <= 0
+// goes to powf (0^0.8 = 0).
+__device__ __forceinline__ float pow_pos(float x, float e) { return x > 0.0f ? __powf(x, e) : powf(x, e); }
 __device__ __forceinline__ float xpow(float x, float e) { return pow_pos(x, e); }
 __device__ __forceinline__ float xmax(float x, float c) { return fmaxf(x, c); }
 __device__ __forceinline__ float xclamp(float x, float lo, float hi) { return clampf(x, lo, hi); }
