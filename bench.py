@@ -58,21 +58,23 @@ BYTES_PER_PARTICLE_STEP = 96  # read 44 B + write 52 B of SoA state, one species
 ADJOINT_HBM_BUDGET = 140e9  # device bytes the batched adjoint may hold (the 150 GB budget, with margin)
 # steps between spatial reorders of the population (one per simulated day at
 # dt 900 s): measured at 10 M particles over 96 steps, a reorder every
-# 12 / 24 / 48 / 96 steps gives 1.059 / 1.079 / 1.097 / 1.103e10
-# particle-steps/s (the kernel averages 0.836 / 0.857 / 0.861 / 0.865 ms as
-# the order decays; a reorder costs 0.92 ms).  The default window of timed
-# steps is one reorder period, and its first step reorders.
+# 24 / 32 / 48 / 96 steps gives 1.297 / 1.318 / 1.324 / 1.335e10
+# particle-steps/s.  A reorder costs about 0.94 ms and the step kernel gains
+# little from it beyond the first step after it (the turbulence mixes the
+# heights within each column at once: 0.626 ms right after a reorder, 0.663
+# ms from the second step on).  The default window of timed steps is one
+# reorder period, and its first step reorders.
 SORT_EVERY = 96
 # DRAM bytes (read + write) per particle of one fused-step launch, from an
 # ncu capture of a 10 M-particle launch of the global run's population
 # (bench.py --quick: particles around the 8 sources, reordered by met cell
-# before the timed steps): 443.3 MB read + 423.3 MB written = 86.7 B per
+# before the timed steps): 443.2 MB read + 421.9 MB written = 86.5 B per
 # particle against the algorithmic 96 B (44 B read, 52 B written); the last
 # ~100 MB of writes are still in the 126 MB L2 when the kernel ends.
-DRAM_BYTES_PER_PARTICLE_NCU = (443.3e6 + 423.3e6) / 10.0e6
+DRAM_BYTES_PER_PARTICLE_NCU = (443.2e6 + 421.9e6) / 10.0e6
 # Warp instructions per 32 particle-steps (smsp__inst_executed.sum of the
-# same capture: 641.5 M for 10 M particles).
-WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 641.5e6 / (10.0e6 / 32)
+# same capture: 581.9 M for 10 M particles).
+WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 581.9e6 / (10.0e6 / 32)
 
 
 def issue_roofline(n_particles, kernel_ms, clk):

@@ -88,6 +88,7 @@ const StepShape kStepShapes[] = {
     {512, 2, 1, fused_step_shape_kernel<512, 2, 1>},
     {256, 6, 1, fused_step_shape_kernel<256, 6, 1>},
     {128, 12, 1, fused_step_shape_kernel<128, 12, 1>},
+    {256, 6, 2, fused_step_shape_kernel<256, 6, 2>},
 };
 constexpr uint32_t kNumStepShapes = sizeof(kStepShapes) / sizeof(kStepShapes[0]);
 
