@@ -192,8 +192,6 @@ def test_met_ring_streaming_gives_identical_results(ctx):
 
 
 def test_device_grid_written_as_netcdf_snapshot(ctx, tmp_path):
-    from scipy.io import netcdf_file
-
     from flexpart_gpu import output
 
     scn = _small(particles=20_000, hours=2)
@@ -206,10 +204,11 @@ def test_device_grid_written_as_netcdf_snapshot(ctx, tmp_path):
     counts, mass, kg = drv.accumulate_concentration_grid(grid, 0, 1e6, scn.outheights)
     path = tmp_path / "grid.nc"
     output.write_grid_netcdf(path, grid, scn.end)
-    with netcdf_file(path, "r", mmap=False) as f:
-        assert np.array_equal(f.variables["concentration_particle_count"][:].reshape(-1), counts.astype(np.int32))
-        assert np.array_equal(f.variables["concentration_mass_kg"][:].reshape(-1), kg)
-        assert f.variables["time"][0] == scn.end
+    v = output.read_netcdf(path)["variables"]
+    assert v["concentration_particle_count"]["data"].dtype == np.uint32
+    assert np.array_equal(v["concentration_particle_count"]["data"].reshape(-1), counts)
+    assert np.array_equal(v["concentration_mass_kg"]["data"].reshape(-1), kg)
+    assert v["time"]["data"].tolist() == [scn.end]
     assert counts.sum() == 20_000
 
 
