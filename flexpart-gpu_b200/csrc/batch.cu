@@ -177,10 +177,11 @@ static_assert(sizeof(kVariants) / sizeof(kVariants[0]) == kNumVariants, "launch 
 
 struct GridConst {
     uint32_t nx, ny, nz, cells;
-    int meters;
+    int meters, sorted;
     float scale;
     uint32_t every;
     float h[FPG_MAX_LEVELS];
+    float lower[kSortedLevels - 1];     // level_sorted's table when `sorted`
 };
 
 __global__ void __launch_bounds__(256) batch_grid_clear_kernel(const BatchState* st, uint32_t every, uint32_t* counts,
@@ -205,7 +206,8 @@ __global__ void __launch_bounds__(256) batch_grid_kernel(const BatchState* st, c
     if (g.every == 0 || (st->step + 1u) % g.every != 0u) return;
     __shared__ float s_h[FPG_MAX_LEVELS];
     __shared__ uint32_t t_key[kTable], t_cnt[kTable], t_mass[kTable];
-    for (uint32_t i = threadIdx.x; i < g.nz; i += blockDim.x) s_h[i] = g.h[i];
+    if (!g.sorted)
+        for (uint32_t i = threadIdx.x; i < g.nz; i += blockDim.x) s_h[i] = g.h[i];
     for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
         t_key[i] = kEmpty;
         t_cnt[i] = 0u;
@@ -225,7 +227,8 @@ __global__ void __launch_bounds__(256) batch_grid_kernel(const BatchState* st, c
             const int32_t cx = (int32_t)F.f[FPG_FIELD_CELL_X][p], cy = (int32_t)F.f[FPG_FIELD_CELL_Y][p];
             const uint32_t ix = (uint32_t)min(max(cx, 0), (int)g.nx - 1);
             const uint32_t iy = (uint32_t)min(max(cy, 0), (int)g.ny - 1);
-            const uint32_t iz = level_of(__uint_as_float(F.f[FPG_FIELD_POS_Z][p]), s_h, g.nz, g.meters);
+            const float z = __uint_as_float(F.f[FPG_FIELD_POS_Z][p]);
+            const uint32_t iz = g.sorted ? level_sorted(z, g.lower, g.nz) : level_of(z, s_h, g.nz, g.meters);
             key = s * g.cells + (ix * g.ny + iy) * g.nz + iz;
             q = quantize(fmaxf(__uint_as_float(F.f[FPG_FIELD_MASS0][p]), 0.0f), g.scale);
         }
@@ -324,6 +327,7 @@ GridConst make_grid_const(const fpg_batch* b) {
     g.cells = g.nx * g.ny * g.nz;
     for (uint32_t k = 0; k < g.nz; ++k) g.h[k] = b->outheights[k];
     g.meters = g.nz > 0 && g.h[g.nz - 1] > 0.0f;
+    g.sorted = sorted_levels(g.h, g.nz, g.lower);
     g.scale = 1.0e6f;
     g.every = b->cfg.output_every_steps;
     return g;

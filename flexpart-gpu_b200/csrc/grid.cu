@@ -20,7 +20,14 @@
 
 namespace fpg {
 
-struct LevelTable { float h[FPG_MAX_LEVELS]; };
+// The output heights: all of them for the scan, and when they are sorted and
+// at most kSortedLevels (`sorted`), the first nz - 1 padded with +inf for the
+// branch-free count (level_sorted).
+struct LevelTable {
+    float h[FPG_MAX_LEVELS];
+    float lower[kSortedLevels - 1];
+    int sorted;
+};
 
 struct GridArgs {
     const int32_t* cell_x; const int32_t* cell_y; const float* pos_z; const uint32_t* flags; const float* mass;
@@ -37,67 +44,78 @@ __device__ __forceinline__ uint32_t cell_of(const GridArgs& a, const float* h, u
     return (ix * a.ny + iy) * a.nz + iz;
 }
 
+// Each thread bins two adjacent slots per pass (one 64-bit load per field).
 constexpr uint32_t kSlotsPerThread = 2;
 
-// Each CTA bins one contiguous chunk of slots, two slots per thread per
-// pass.  The fields of the next pass are loaded before the current pass's
-// run sums and table updates, so a thread always has a pass of loads in
-// flight.  All sums are u32, so the grid does not depend on the order of
-// the additions.
-struct SlotFields {
-    uint32_t f[kSlotsPerThread];
-    int32_t cx[kSlotsPerThread], cy[kSlotsPerThread];
-    float z[kSlotsPerThread], m[kSlotsPerThread];
+struct SlotPair {
+    uint2 f, cx, cy, z, m;      // flags, cell_x, cell_y, pos_z, mass (bits)
 };
 
-__device__ __forceinline__ void load_pass(const GridArgs& a, uint64_t base, uint64_t end, SlotFields& s) {
-#pragma unroll
-    for (int j = 0; j < (int)kSlotsPerThread; ++j) {
-        const uint64_t p = base + (uint64_t)j * blockDim.x + threadIdx.x;
-        s.f[j] = 0u;
-        if (p < end) {
-            s.f[j] = a.flags[p];
-            s.cx[j] = a.cell_x[p];
-            s.cy[j] = a.cell_y[p];
-            s.z[j] = a.pos_z[p];
-            s.m[j] = a.mass[p];
-        }
+__device__ __forceinline__ void load_pair(const GridArgs& a, uint64_t p, uint64_t end, SlotPair& s) {
+    s.f = make_uint2(0u, 0u);
+    if (p + 1u < end) {
+        s.f = *reinterpret_cast<const uint2*>(a.flags + p);
+        s.cx = *reinterpret_cast<const uint2*>(a.cell_x + p);
+        s.cy = *reinterpret_cast<const uint2*>(a.cell_y + p);
+        s.z = *reinterpret_cast<const uint2*>(a.pos_z + p);
+        s.m = *reinterpret_cast<const uint2*>(a.mass + p);
+    } else if (p < end) {
+        s.f.x = a.flags[p];
+        s.cx.x = (uint32_t)a.cell_x[p];
+        s.cy.x = (uint32_t)a.cell_y[p];
+        s.z.x = __float_as_uint(a.pos_z[p]);
+        s.m.x = __float_as_uint(a.mass[p]);
     }
 }
 
+// The cell and the scaled mass of one slot (kEmpty and 0 when inactive).
+__device__ __forceinline__ void slot_cell(const GridArgs& a, const LevelTable& lt, const float* s_h, uint32_t f,
+                                          uint32_t cx, uint32_t cy, uint32_t zb, uint32_t mb, uint32_t& key,
+                                          uint32_t& q) {
+    key = kEmpty;
+    q = 0u;
+    if (f & 1u) {
+        const uint32_t ix = (uint32_t)min(max((int32_t)cx, 0), (int)a.nx - 1);
+        const uint32_t iy = (uint32_t)min(max((int32_t)cy, 0), (int)a.ny - 1);
+        const float z = __uint_as_float(zb);
+        const uint32_t iz = lt.sorted ? level_sorted(z, lt.lower, a.nz) : level_of(z, s_h, a.nz, a.meters);
+        key = (ix * a.ny + iy) * a.nz + iz;
+        q = quantize(fmaxf(__uint_as_float(mb), 0.0f), a.mass_scale);
+    }
+}
+
+// Each CTA bins one contiguous chunk of slots.  The fields of the next pass
+// are loaded before the current pass's warp sums and table updates, so a
+// thread always has a pass of loads in flight.  A warp sums the runs of equal
+// cells of its 32 even slots, then of its 32 odd ones (the reorder keeps
+// neighbouring slots in one cell, so both stay long).  All sums are u32, so
+// the grid does not depend on the order of the additions.
 __global__ void __launch_bounds__(256) grid_kernel(GridArgs a, LevelTable lt, uint32_t chunk,
                                                    uint32_t* __restrict__ counts, uint32_t* __restrict__ mass) {
     __shared__ float s_h[FPG_MAX_LEVELS];
     __shared__ uint32_t t_key[kTable], t_cnt[kTable], t_mass[kTable];
-    for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_h[i] = lt.h[i];
+    if (!lt.sorted)
+        for (uint32_t i = threadIdx.x; i < a.nz; i += blockDim.x) s_h[i] = lt.h[i];
     for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
         t_key[i] = kEmpty;
         t_cnt[i] = 0u;
         t_mass[i] = 0u;
     }
     const unsigned lane = threadIdx.x & 31u;
-    const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+    const uint64_t begin = (uint64_t)blockIdx.x * chunk;    // chunk: a multiple of the pass, so begin is even
     const uint64_t end = min(begin + chunk, (uint64_t)a.n);
     const uint64_t pass = (uint64_t)kSlotsPerThread * blockDim.x;
-    SlotFields cur;
-    load_pass(a, begin, end, cur);
+    const uint64_t mine = (uint64_t)kSlotsPerThread * threadIdx.x;
+    SlotPair cur;
+    load_pair(a, begin + mine, end, cur);
     __syncthreads();
     for (uint64_t base = begin; base < end; base += pass) {      // uniform across the CTA
-        uint32_t key[kSlotsPerThread], q[kSlotsPerThread];
-#pragma unroll
-        for (int j = 0; j < (int)kSlotsPerThread; ++j) {
-            key[j] = kEmpty;
-            q[j] = 0u;
-            if (cur.f[j] & 1u) {
-                const uint32_t ix = (uint32_t)min(max(cur.cx[j], 0), (int)a.nx - 1);
-                const uint32_t iy = (uint32_t)min(max(cur.cy[j], 0), (int)a.ny - 1);
-                key[j] = (ix * a.ny + iy) * a.nz + level_of(cur.z[j], s_h, a.nz, a.meters);
-                q[j] = quantize(fmaxf(cur.m[j], 0.0f), a.mass_scale);
-            }
-        }
-        if (base + pass < end) load_pass(a, base + pass, end, cur);
-#pragma unroll
-        for (int j = 0; j < (int)kSlotsPerThread; ++j) warp_runs_add(key[j], q[j], lane, t_key, t_cnt, t_mass, counts, mass);
+        uint32_t k0, q0, k1, q1;
+        slot_cell(a, lt, s_h, cur.f.x, cur.cx.x, cur.cy.x, cur.z.x, cur.m.x, k0, q0);
+        slot_cell(a, lt, s_h, cur.f.y, cur.cx.y, cur.cy.y, cur.z.y, cur.m.y, k1, q1);
+        if (base + pass < end) load_pair(a, base + pass + mine, end, cur);
+        warp_runs_add(k0, q0, lane, t_key, t_cnt, t_mass, counts, mass);      // the even slots' runs
+        warp_runs_add(k1, q1, lane, t_key, t_cnt, t_mass, counts, mass);      // the odd slots'
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < kTable; i += blockDim.x) {
@@ -127,6 +145,7 @@ static fpg_status prepare(const fpg_particles* P, const fpg_grid* g, uint32_t sp
     if (P->dispatch > (size_t)UINT32_MAX) return FPG_ERR_VALUE_TOO_LARGE;
     std::memset(&lt, 0, sizeof(lt));
     if (oh) std::memcpy(lt.h, oh, g->nz * sizeof(float));
+    lt.sorted = sorted_levels(lt.h, (uint32_t)g->nz, lt.lower);
     a.cell_x = (const int32_t*)P->field[FPG_FIELD_CELL_X];
     a.cell_y = (const int32_t*)P->field[FPG_FIELD_CELL_Y];
     a.pos_z = (const float*)P->field[FPG_FIELD_POS_Z];

@@ -4,6 +4,7 @@
 // grid.cu and batch.cu.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -19,6 +20,30 @@ __device__ __forceinline__ uint32_t level_of(float z, const float* h, uint32_t n
     // u32(clamp(i32(floor(z)), 0, nz-1)); float->int conversion saturates
     const int iz = (int)floorf(z);
     return (uint32_t)min(max(iz, 0), (int)nz - 1);
+}
+
+// pos_z_to_level for output heights in ascending order, at most
+// kSortedLevels of them, branch-free: the first k with z <= h[k] is the
+// number of the first nz - 1 heights below z, which `lower` holds padded
+// with +inf up to kSortedLevels - 1 entries; a NaN height (no k) is the top
+// level, as in the scan.
+constexpr uint32_t kSortedLevels = 8;
+
+__device__ __forceinline__ uint32_t level_sorted(float z, const float (&lower)[kSortedLevels - 1], uint32_t nz) {
+    uint32_t k = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < kSortedLevels - 1; ++i) k += lower[i] < z ? 1u : 0u;
+    return z == z ? k : nz - 1u;
+}
+
+// Host side: whether level_sorted applies to the output heights h[0..nz)
+// (metres, ascending, at most kSortedLevels), and its padded table.
+inline int sorted_levels(const float* h, uint32_t nz, float (&lower)[kSortedLevels - 1]) {
+    int sorted = nz > 0 && nz <= kSortedLevels && h[nz - 1] > 0.0f;
+    for (uint32_t k = 1; sorted && k < nz; ++k)
+        if (!(h[k] >= h[k - 1])) sorted = 0;
+    for (uint32_t k = 0; k < kSortedLevels - 1; ++k) lower[k] = k + 1 < nz ? h[k] : INFINITY;
+    return sorted;
 }
 
 // quantize_mass_to_u32 (concentration_gridding.wgsl:317-326).

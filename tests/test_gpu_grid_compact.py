@@ -39,7 +39,10 @@ def test_gridding_reference_case(ctx):
     assert np.array_equal(kg, (om.astype(np.float32) / np.float32(1e6)).astype(np.float32))
 
 
-@pytest.mark.parametrize("outheights", [[100.0, 500.0, 1000.0], [0.0, 0.0, 0.0, 0.0]])
+@pytest.mark.parametrize("outheights", [[100.0, 500.0, 1000.0], [0.0, 0.0, 0.0, 0.0],
+                                        [500.0, 100.0, 1000.0],                      # unsorted: the scan
+                                        [50.0 * (k + 1) for k in range(12)],         # sorted, beyond the count
+                                        [100.0, 100.0, 400.0, 400.0, 800.0, 1600.0, 3200.0, 6400.0]])
 def test_gridding_bit_exact_large(ctx, outheights):
     nx, ny = 40, 30
     rec = population(nx, ny, 200_003, seed=3, z_max=2000.0 if outheights[0] > 0 else 5.0)
