@@ -6,15 +6,19 @@
 // as written, and the only fused operation is the explicit fmaf of lerp()
 // (the reference CPU lerp is `a.mul_add(1 - t, b * t)`,
 // src/physics/interpolation.rs:75-77, src/io/temporal.rs:417-420).
-// Transcendentals are CUDA's accurate expf/logf/exp2f/log2f/sincosf/cbrtf
-// (no fast-math intrinsics); sqrtf is correctly rounded, and '/' is too
-// except in the step's units (step.cu, batch.cu, adjoint.cu), which the
-// build compiles with the approximate full-range division (within 2 ulp) and
-// with subnormal values flushed to zero.
+// Transcendentals: cbrtf and expf (deposition) as CUDA computes them; the
+// Hanna and Langevin exponentials and powers at the accuracy WGSL specifies
+// for the reference's shaders (__expf, __powf); the Box-Muller logarithm,
+// sine and cosine of box_muller_math.h.  sqrtf is correctly rounded, and
+// '/' is too except in the step's units (step.cu, batch.cu, adjoint.cu),
+// which the build compiles with the approximate full-range division (within
+// 2 ulp) and with subnormal values flushed to zero.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
+
+#include "box_muller_math.h"
 
 namespace fpg {
 
@@ -81,17 +85,18 @@ __device__ __forceinline__ u32x4 counter_add(u32x4 b, uint32_t offset) {
 // u32_to_uniform01 (rng.rs:94-96).
 __device__ __forceinline__ float u32_to_uniform01(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216.0f); }
 
-// box_muller_normals (physics/langevin.rs:176-182, langevin_fused.wgsl:186-192).
-// sincosf shares one argument reduction between the sine and the cosine; its
-// results are those of sinf and cosf (checked bit for bit over 2.4e7 angles
-// of the step), at 2.6 % less step time.
+// box_muller_normals (physics/langevin.rs:176-182, langevin_fused.wgsl:186-192),
+// with the logarithm and the sine and cosine of box_muller_math.h: written
+// for these inputs (u0 in {FLT_MIN} and [2^-24, 1 - 2^-24], theta = 2pi u1
+// in [0, 2pi)), within 1.5 ulp of the exact values, and closer to the libm
+// results of the reference's CPU path than CUDA's logf and sincosf.
 __device__ __forceinline__ float2 box_muller(float u0, float u1) {
     const float ru = clampf(u0, 1.17549435e-38f, 0.99999994f);
     const float au = clampf(u1, 0.0f, 0.99999994f);
-    const float radius = sqrtf(-2.0f * logf(ru));
+    const float radius = sqrtf(-2.0f * bm_log(ru));
     const float theta = 6.2831855f * au;
     float sn, cs;
-    sincosf(theta, &sn, &cs);
+    bm_sincos(theta, &sn, &cs);
     return make_float2(radius * cs, radius * sn);
 }
 
