@@ -702,7 +702,7 @@ extern "C" fpg_status fpg_batch_run_sequential(fpg_batch* b, uint32_t n_steps) {
             a.alpha = alpha;
             a.key0 = d.key0; a.key1 = d.key1;
             a.counter = counter;
-            fused_step_kernel<<<(released + 255) / 256, 256, level_smem_bytes(b->met), s>>>(a);
+            fused_step_kernel<<<(released + 255) / 256, 256, 0, s>>>(a);
             b->ctx->count();
         }
         enqueue_post(b, s);

@@ -42,12 +42,7 @@
 namespace fpg {
 
 __global__ void __launch_bounds__(256, 5) fused_step_kernel(StepArgs a) {
-    extern __shared__ float s_levels[];
-    Levels lv{};
-    if (a.stages & FPG_STAGE_ADVECT) {
-        lv = stage_levels(a, s_levels);
-        __syncthreads();
-    }
+    const Levels lv = global_levels(a);
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     particle_step(a, lv, p, p, a.alpha, a.counter, a.key0, a.key1);
@@ -55,13 +50,17 @@ __global__ void __launch_bounds__(256, 5) fused_step_kernel(StepArgs a) {
 
 // The same pass under another launch shape: BLOCK threads per CTA compiled
 // for MINB resident CTAs per SM, PPT particles per thread (slots of one CTA
-// are contiguous; thread t takes t, t + BLOCK, ...).  Each particle's
+// are contiguous; thread t takes t, t + BLOCK, ...); with several particles
+// per thread the CTA stages the level heights in shared memory once (the
+// global pointers would cost registers across the loop).  Each particle's
 // arithmetic is the same, so the results are too.
 template <int BLOCK, int MINB, int PPT>
 __global__ void __launch_bounds__(BLOCK, MINB) fused_step_shape_kernel(StepArgs a) {
     extern __shared__ float s_levels[];
     Levels lv{};
-    if (a.stages & FPG_STAGE_ADVECT) {
+    if constexpr (PPT == 1) {
+        lv = global_levels(a);
+    } else if (a.stages & FPG_STAGE_ADVECT) {
         lv = stage_levels(a, s_levels);
         __syncthreads();
     }
@@ -575,7 +574,7 @@ extern "C" fpg_status fpg_step(fpg_ctx* ctx, fpg_particles* P, const fpg_met* me
 
     cudaStream_t s = ctx->pick(stream);
     const StepShape& sh = kStepShapes[ctx->step_shape < kNumStepShapes ? ctx->step_shape : 0];
-    sh.kernel<<<blocks_for(n, sh.block * sh.ppt), sh.block, smem, s>>>(a);
+    sh.kernel<<<blocks_for(n, sh.block * sh.ppt), sh.block, sh.ppt > 1 ? smem : 0, s>>>(a);
     ctx->count();
     FPG_CHECK_LAUNCH();
     if (turb && next_counter) {

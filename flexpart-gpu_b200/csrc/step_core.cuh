@@ -60,8 +60,9 @@ inline int level_mode(const fpg_met* m) {
     return m->level_table ? LEVELS_TABLE : m->monotonic ? LEVELS_BISECT : LEVELS_SCAN;
 }
 
-// The level heights and the bucket table as a kernel staged them in shared
-// memory (stage_levels).
+// The level heights and the bucket table where a kernel reads them: in
+// global memory through L1 (global_levels), or staged in shared memory
+// (stage_levels).
 struct Levels {
     const float* h;
     const uint8_t* tab;
@@ -69,6 +70,12 @@ struct Levels {
     uint32_t nz;
     int has, mode;
 };
+
+// The met's own arrays (a kernel with one particle per thread: every CTA
+// would otherwise stage them for its 256 particles and wait at a barrier).
+__device__ __forceinline__ Levels global_levels(const StepArgs& a) {
+    return Levels{a.heights, a.level_table, a.level_inv_w, a.nz, a.has_heights, a.level_mode};
+}
 
 // Copies the level heights (and the bucket table) into shared memory at
 // `smem` (level_smem_bytes of the met); the caller synchronises the block.
