@@ -879,10 +879,9 @@ def main():
     state = {"bracket": None, "counter": counter, "t": drv.current_time_seconds, "k": 0}
 
     def set_bracket(fa, fb):
-        for which, fi in ((0, fa), (1, fb)):
-            u, v, w = frame_dev[fi]
-            api.check(lib.fpg_met_upload_frame_device(met.h, which, ctypes.c_void_p(u.ptr), ctypes.c_void_p(v.ptr),
-                                                      ctypes.c_void_p(w.ptr), None), "met frame")
+        (u0, v0, w0), (u1, v1, w1) = frame_dev[fa], frame_dev[fb]
+        api.check(lib.fpg_met_upload_bracket_device(met.h, *(ctypes.c_void_p(x.ptr) for x in (u0, v0, w0, u1, v1, w1)),
+                                                    None), "met bracket")
         for which, fi in ((0, fa), (1, fb)):
             api.check(lib.fpg_surface_upload(surf.h, which, ctypes.c_void_p(surf_dev[fi].ptr), None), "surface")
         api.check(lib.fpg_cellfield_from_precipitation(wet.h, ctypes.c_void_p(precip_dev[fa].ptr), None, None,

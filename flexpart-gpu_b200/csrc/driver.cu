@@ -385,12 +385,14 @@ static fpg_status bracket_from_ring(fpg_forward* d, int64_t t0, int64_t t1) {
     cudaStream_t s = d->ctx->stream;
     const size_t nodes = d->met->nx * d->met->ny * d->met->nz, cells = d->met->nx * d->met->ny;
     const int idx[2] = {i0, i1};
+    for (int which = 0; which < 2; ++which) FPG_CUDA(cudaStreamWaitEvent(s, d->ring[idx[which]].copied, 0));
+    const float* f0 = d->ring[i0].uvw;
+    const float* f1 = d->ring[i1].uvw;
+    fpg_status st = fpg_met_upload_bracket_device(d->met, f0, f0 + nodes, f0 + 2 * nodes, f1, f1 + nodes,
+                                                  f1 + 2 * nodes, nullptr);
+    if (st != FPG_OK) return st;
     for (int which = 0; which < 2; ++which) {
         fpg_forward::MetSlot& slot = d->ring[idx[which]];
-        FPG_CUDA(cudaStreamWaitEvent(s, slot.copied, 0));
-        fpg_status st = fpg_met_upload_frame_device(d->met, which, slot.uvw, slot.uvw + nodes, slot.uvw + 2 * nodes,
-                                                    nullptr);
-        if (st != FPG_OK) return st;
         FPG_CUDA(cudaMemcpyAsync(d->surface->frame[which], slot.surface, cells * sizeof(fpg_surface_cell),
                                  cudaMemcpyDeviceToDevice, s));
         d->surface->uploaded[which] = true;

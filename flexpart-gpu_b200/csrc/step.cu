@@ -124,6 +124,18 @@ __global__ void __launch_bounds__(256) pack_frame_kernel(const float* __restrict
     node[4 + which] = w[n];
 }
 
+// Both frames of a bracket into whole nodes: 24 B read and 32 B written per
+// node, where two pack_frame_kernel passes each read the node's other lanes
+// back before their partial stores.
+__global__ void __launch_bounds__(256) pack_bracket_kernel(const float* __restrict__ u0, const float* __restrict__ v0,
+                                                           const float* __restrict__ w0, const float* __restrict__ u1,
+                                                           const float* __restrict__ v1, const float* __restrict__ w1,
+                                                           uint32_t nodes, float4* bracket) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nodes) return;
+    st_node(bracket, n, make_float4(u0[n], v0[n], w0[n], 0.0f), make_float4(u1[n], v1[n], w1[n], 0.0f));
+}
+
 // wet_precipitation_state + below_cloud_scavenging_coefficient_gas
 // (physics/wet_scavenging.rs:179-225,78-82) per met cell.
 __global__ void __launch_bounds__(256) wet_cells_kernel(const float* __restrict__ lsp_in,
@@ -222,6 +234,19 @@ extern "C" fpg_status fpg_met_upload_frame_device(fpg_met* m, int32_t which, con
                                                   const float* w, void* stream) {
     if (!m || !u || !v || !w || (which != 0 && which != 1)) return FPG_ERR_INVALID_ARGUMENT;
     return met_pack(m, which, u, v, w, m->ctx->pick(stream));
+}
+
+extern "C" fpg_status fpg_met_upload_bracket_device(fpg_met* m, const float* u0, const float* v0, const float* w0,
+                                                    const float* u1, const float* v1, const float* w1,
+                                                    void* stream) {
+    if (!m || !u0 || !v0 || !w0 || !u1 || !v1 || !w1) return FPG_ERR_INVALID_ARGUMENT;
+    const uint32_t nodes = (uint32_t)(m->nx * m->ny * m->nz);
+    pack_bracket_kernel<<<blocks_for(nodes, 256), 256, 0, m->ctx->pick(stream)>>>(u0, v0, w0, u1, v1, w1, nodes,
+                                                                                   m->bracket);
+    m->ctx->count();
+    FPG_CHECK_LAUNCH();
+    m->uploaded[0] = m->uploaded[1] = true;
+    return FPG_OK;
 }
 
 extern "C" fpg_status fpg_met_set_level_heights(fpg_met* m, const float* heights, size_t n) {

@@ -75,6 +75,7 @@ _sig("fpg_met_create", _i32, _vp, _sz, _sz, _sz, ctypes.POINTER(_vp))
 _sig("fpg_met_destroy", _i32, _vp)
 _sig("fpg_met_upload_frame", _i32, _vp, _i32, _vp, _vp, _vp, _vp)
 _sig("fpg_met_upload_frame_device", _i32, _vp, _i32, _vp, _vp, _vp, _vp)
+_sig("fpg_met_upload_bracket_device", _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
 _sig("fpg_met_set_level_heights", _i32, _vp, _vp, _sz)
 _sig("fpg_pbl_create", _i32, _vp, _sz, _sz, ctypes.POINTER(_vp))
 _sig("fpg_pbl_destroy", _i32, _vp)
@@ -192,6 +193,7 @@ EXPORTED = [
     "fpg_particles_download", "fpg_particles_field", "fpg_particles_copy_field",
     "fpg_step_tuning_candidates", "fpg_step_autotune", "fpg_step_set_tuning", "fpg_step_get_tuning",
     "fpg_met_create", "fpg_met_destroy", "fpg_met_upload_frame", "fpg_met_upload_frame_device",
+    "fpg_met_upload_bracket_device",
     "fpg_met_set_level_heights",
     "fpg_pbl_create", "fpg_pbl_destroy", "fpg_pbl_upload", "fpg_pbl_download",
     "fpg_surface_create", "fpg_surface_destroy", "fpg_surface_upload", "fpg_pbl_diagnostics",

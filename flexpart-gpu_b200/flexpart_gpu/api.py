@@ -188,6 +188,17 @@ class Met:
         check(lib.fpg_met_upload_frame(self.h, which, *[_p(a) for a in arrs], None), "fpg_met_upload_frame")
         self.ctx.synchronize()
 
+    def upload_bracket_device(self, frame0, frame1, stream=None):
+        """Both frames from device arrays ((u, v, w) DeviceArrays each) in one
+        pass (fpg_met_upload_bracket_device)."""
+        n = self.shape[0] * self.shape[1] * self.shape[2]
+        ptrs = []
+        for a in (*frame0, *frame1):
+            if a.n != n:
+                raise ValueError("wind frame size does not match the met shape")
+            ptrs.append(ctypes.c_void_p(a.ptr))
+        check(lib.fpg_met_upload_bracket_device(self.h, *ptrs, stream), "fpg_met_upload_bracket_device")
+
     def set_level_heights(self, heights):
         h = np.ascontiguousarray(heights, np.float32)
         check(lib.fpg_met_set_level_heights(self.h, _p(h), h.size), "fpg_met_set_level_heights")

@@ -217,6 +217,13 @@ fpg_status fpg_met_upload_frame(fpg_met* m, int32_t which, const float* u, const
 /* Same from device arrays (already resident frames, e.g. a frame ring). */
 fpg_status fpg_met_upload_frame_device(fpg_met* m, int32_t which, const float* u_dev,
                                        const float* v_dev, const float* w_dev, void* stream);
+/* Both frames of a new bracket from device arrays in one pass
+ * (upload_dual_wind_if_bracket_changed, src/simulation/timeloop.rs:1378-1402,
+ * uploads t0 and t1 together): the same bracket as two
+ * fpg_met_upload_frame_device calls, writing each node whole. */
+fpg_status fpg_met_upload_bracket_device(fpg_met* m, const float* u0_dev, const float* v0_dev,
+                                         const float* w0_dev, const float* u1_dev, const float* v1_dev,
+                                         const float* w1_dev, void* stream);
 /* VelocityToGridScale::level_heights_m (advection.rs:31-41): heights [m] of
  * the nz wind levels.  All-zero (top <= 0) selects the legacy mode where
  * pos_z is a level index.  n must equal nz (n <= FPG_MAX_LEVELS). */

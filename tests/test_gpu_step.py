@@ -166,6 +166,25 @@ def test_level_table_search_matches_the_scan(ctx, kind):
     _compare_state(p.download(), s, kind, rec, s64)
 
 
+def test_bracket_upload_in_one_pass_matches_two_frame_uploads(ctx):
+    """fpg_met_upload_bracket_device (both frames, whole nodes) gives the
+    bracket of two fpg_met_upload_frame calls: the same step, bit for bit,
+    also after a bracket uploaded the other way round first."""
+    spec, frames, met = small_met()
+    rec = population(spec.nx, spec.ny, 30_001, seed=5)
+    m, surf, pbl, p = _gpu_setup(ctx, spec, frames, met, 0.3, rec)
+    prm = production_params(alpha=0.3, counter=(4, 0, 0, 0))
+    api.step(ctx, p, m, pbl, prm)
+    want = p.download()
+    dev = [api.DeviceArray.from_numpy(ctx, np.ascontiguousarray(met[k], np.float32).reshape(-1))
+           for k in ("u0", "v0", "w0", "u1", "v1", "w1")]
+    m.upload_bracket_device(dev[3:], dev[:3])          # swapped frames first: every node rewritten
+    m.upload_bracket_device(dev[:3], dev[3:])
+    p.upload(rec)
+    api.step(ctx, p, m, pbl, prm)
+    assert p.download().tobytes() == want.tobytes()
+
+
 def test_launch_shapes_give_the_same_bits_and_the_tuner_restores_the_state(ctx):
     """Every compiled launch shape of fpg_step (block size, resident blocks,
     particles per thread) gives the default shape's results bit for bit;
