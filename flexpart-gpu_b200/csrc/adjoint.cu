@@ -174,37 +174,29 @@ __global__ void inverse_snapshot_kernel(const BatchState* st, const ScenDev* __r
 // whose last receptor hit came before this step has a zero adjoint from this
 // step on, so its tape is never read -- it is marked inactive for the
 // reverse and not stepped.
+// One CTA per 256-slot work item, launched over all items; the level arrays
+// are read from global memory (no staging, no barrier).
 __global__ void __launch_bounds__(256, 4) inverse_tape_kernel(StepArgs a, const BatchState* st,
                                                               const ScenDev* __restrict__ sc,
                                                               const uint2* __restrict__ items, uint32_t n_items,
-                                                              uint32_t* work, TapeBase tb, uint32_t every,
+                                                              TapeBase tb, uint32_t every,
                                                               const uint32_t* __restrict__ live) {
-    extern __shared__ float s_levels[];
-    __shared__ uint32_t s_item;
-    const Levels lv = stage_levels(a, s_levels);
-    const float alpha = st->alpha;
+    if (blockIdx.x >= n_items) return;
+    const uint2 w = items[blockIdx.x];
+    const ScenDev& d = sc[w.x];
+    const uint32_t local = w.y + threadIdx.x;
+    if (local >= d.released) return;
     const uint32_t slice = st->step % tb.slices;
     TapeRec rec;
     rec.output = every != 0 && (st->step + 1u) % every == 0u;
 #pragma unroll
     for (int f = 0; f < TAPE_FIELDS; ++f) rec.t.f[f] = tb.field(slice, f);
-    for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0) s_item = atomicAdd(work, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
-        if (it >= n_items) break;
-        const uint2 w = items[it];
-        const ScenDev& d = sc[w.x];
-        const uint32_t local = w.y + threadIdx.x;
-        if (local >= d.released) continue;
-        const uint32_t p = d.offset + local;
-        if (!(a.flags[p] & FLAG_ACTIVE) || (live && live[p] <= st->step)) {
-            reinterpret_cast<uint32_t*>(rec.t.f[T_FLAGS])[p] = 0u;
-            continue;
-        }
-        particle_step_t<TapeRec>(a, lv, p, local, alpha, d.counter, d.key0, d.key1, rec);
+    const uint32_t p = d.offset + local;
+    if (!(a.flags[p] & FLAG_ACTIVE) || (live && live[p] <= st->step)) {
+        reinterpret_cast<uint32_t*>(rec.t.f[T_FLAGS])[p] = 0u;
+        return;
     }
+    particle_step_t<TapeRec>(a, global_levels(a), p, local, st->alpha, d.counter, d.key0, d.key1, rec);
 }
 
 // ---- reverse ----------------------------------------------------------------------
@@ -570,13 +562,12 @@ struct InverseData {
     double* dsrc = nullptr;
     uint2* items = nullptr;              // 256-slot work items
     uint32_t n_items = 0;
-    uint32_t* work = nullptr;
     uint32_t* work_rev = nullptr;        // one work counter per tape slice for the reverse sweep
     // start time of the met bracket packed in device memory (INT64_MIN: unknown)
     int64_t packed_ta = INT64_MIN;
     bool forward_done = false;
     uint64_t bytes = 0;
-    uint32_t grid_tape = 0, grid_adj = 0;  // persistent grids: SMs x resident CTAs
+    uint32_t grid_adj = 0;               // the reverse's persistent grid: SMs x resident CTAs
     // one taped step (pre, snapshot, tape pass, [sampling], end), captured
     cudaGraph_t tape_graph[2] = {nullptr, nullptr};
     cudaGraphExec_t tape_exec[2] = {nullptr, nullptr};
@@ -630,11 +621,9 @@ static void enqueue_taped_step(fpg_inverse* v, bool sample, cudaStream_t s) {
     InverseData& d = v->d;
     enqueue_pre(b, s);
     inverse_snapshot_kernel<<<1, 256, 0, s>>>(b->st, b->sc, (uint32_t)b->scen.size(), d.slices, d.st_all, d.sc_all);
-    cudaMemsetAsync(d.work, 0, 4, s);
-    inverse_tape_kernel<<<d.grid_tape, 256, level_smem_bytes(b->met), s>>>(make_step_args(b), b->st, b->sc,
-                                                                             d.items, d.n_items, d.work,
-                                                                             tape_base(v), d.cfg.sample_every_steps,
-                                                                             sample ? nullptr : d.last_hit);
+    inverse_tape_kernel<<<std::max(d.n_items, 1u), 256, 0, s>>>(make_step_args(b), b->st, b->sc, d.items, d.n_items,
+                                                                tape_base(v), d.cfg.sample_every_steps,
+                                                                sample ? nullptr : d.last_hit);
     b->ctx->count(2);
     if (sample) enqueue_inverse_sample(b, s);
     enqueue_end(b, s);
@@ -716,7 +705,7 @@ extern "C" fpg_status fpg_inverse_destroy(fpg_inverse* v) {
     cudaFree(d.rmap); cudaFree(d.sim); cudaFree(d.last_hit); cudaFree(d.g); cudaFree(d.ring_raw); cudaFree(d.bias);
     cudaFree(d.ckpt); cudaFree(d.ckpt_st); cudaFree(d.ckpt_sc); cudaFree(d.st_all); cudaFree(d.sc_all);
     cudaFree(d.tape); cudaFree(d.lam); cudaFree(d.dbias); cudaFree(d.dbias_f); cudaFree(d.dsrc);
-    cudaFree(d.items); cudaFree(d.work); cudaFree(d.work_rev);
+    cudaFree(d.items); cudaFree(d.work_rev);
     fpg_batch_destroy(v->b);
     delete v;
     return FPG_OK;
@@ -789,7 +778,6 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = alloc((void**)&d.dbias_f, d.nodes * 3 * 4);
     if (e == cudaSuccess) e = alloc((void**)&d.dsrc, n_src * 4 * 8);
     if (e == cudaSuccess) e = alloc((void**)&d.items, items.size() * sizeof(uint2));
-    if (e == cudaSuccess) e = alloc((void**)&d.work, 4);
     if (e == cudaSuccess) e = alloc((void**)&d.work_rev, (size_t)S * 4);
     cudaStream_t s = ctx->stream;
     if (e == cudaSuccess) e = cudaMemcpyAsync(d.rmap, rmap.data(), rmap.size() * 4, cudaMemcpyHostToDevice, s);
@@ -798,10 +786,7 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
     if (e == cudaSuccess) e = cudaMemsetAsync(d.bias, 0, d.nodes * 3 * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d.ring_raw, 0, d.nodes * bc.n_frames * sizeof(float4), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    int per_sm_tape = 0, per_sm_adj = 0;
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tape, inverse_tape_kernel, 256,
-                                                          nz * sizeof(float) + FPG_LEVEL_BUCKETS);
+    int per_sm_adj = 0;
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adj, inverse_adjoint_kernel, 256,
                                                           nz * sizeof(float) + FPG_LEVEL_BUCKETS);
@@ -809,7 +794,6 @@ extern "C" fpg_status fpg_inverse_create(fpg_ctx* ctx, const fpg_inverse_config*
         fpg_inverse_destroy(v);
         return cuda_status(e);
     }
-    d.grid_tape = (uint32_t)ctx->sm_count * (uint32_t)std::max(per_sm_tape, 1);
     d.grid_adj = (uint32_t)ctx->sm_count * (uint32_t)std::max(per_sm_adj, 1);
     b->inv = &d;
     *out = v;

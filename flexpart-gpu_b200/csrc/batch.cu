@@ -161,7 +161,25 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_step_kernel(StepArgs a, Bat
     }
 }
 
-// The launch shapes the persistent step is compiled for; the tuner picks one.
+// The same pass with one CTA per work item of BLOCK slots, launched over all
+// items (particles_per_thread 0 in the tuning records): no work counter and
+// no barrier, the level arrays read from global memory, and the hardware's
+// block scheduler spreading the items of small and large scenarios.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) batch_step_flat_kernel(StepArgs a, BatchState* st,
+                                                                      const ScenDev* __restrict__ sc,
+                                                                      const uint2* __restrict__ items,
+                                                                      uint32_t n_items) {
+    if (blockIdx.x >= n_items) return;
+    const uint2 w = items[blockIdx.x];
+    const ScenDev& d = sc[w.x];
+    const uint32_t local = w.y + threadIdx.x;
+    if (local < d.released)
+        particle_step(a, global_levels(a), d.offset + local, local, st->alpha, d.counter, d.key0, d.key1);
+}
+
+// The launch shapes the particle pass is compiled for; the tuner picks one.
+// ppt 0: batch_step_flat_kernel, one CTA per item of `block` slots.
 struct StepVariant {
     uint32_t block, minb, ppt;
     void (*kernel)(StepArgs, BatchState*, const ScenDev*, const uint2*, uint32_t);
@@ -172,6 +190,8 @@ const StepVariant kVariants[] = {
     {256, 3, 1, batch_step_kernel<256, 3, 1>}, {256, 2, 1, batch_step_kernel<256, 2, 1>},
     {128, 8, 1, batch_step_kernel<128, 8, 1>}, {128, 8, 2, batch_step_kernel<128, 8, 2>},
     {512, 2, 1, batch_step_kernel<512, 2, 1>}, {256, 5, 1, batch_step_kernel<256, 5, 1>},
+    {256, 5, 0, batch_step_flat_kernel<256, 5>}, {128, 10, 0, batch_step_flat_kernel<128, 10>},
+    {128, 12, 0, batch_step_flat_kernel<128, 12>},
 };
 static_assert(sizeof(kVariants) / sizeof(kVariants[0]) == kNumVariants, "launch shape table");
 
@@ -383,8 +403,12 @@ void enqueue_end(fpg_batch* b, cudaStream_t s) {
 void enqueue_step_kernel(fpg_batch* b, cudaStream_t s) {
     const StepVariant& v = kVariants[b->variant];
     const StepArgs a = make_step_args(b);
-    const uint32_t grid = (uint32_t)b->ctx->sm_count * std::max(b->resident[b->variant], 1u);
-    v.kernel<<<grid, v.block, level_smem_bytes(b->met), s>>>(a, b->st, b->sc, b->items, b->n_items);
+    if (v.ppt == 0) {
+        v.kernel<<<std::max(b->n_items, 1u), v.block, 0, s>>>(a, b->st, b->sc, b->items, b->n_items);
+    } else {
+        const uint32_t grid = (uint32_t)b->ctx->sm_count * std::max(b->resident[b->variant], 1u);
+        v.kernel<<<grid, v.block, level_smem_bytes(b->met), s>>>(a, b->st, b->sc, b->items, b->n_items);
+    }
     b->ctx->count(1);
 }
 
@@ -396,7 +420,7 @@ void enqueue_batched_step(fpg_batch* b, cudaStream_t s) {
 
 // Work items of shape `v`: every scenario cut into chunks of block * ppt slots.
 fpg_status build_items(fpg_batch* b, uint32_t v) {
-    const uint32_t chunk = kVariants[v].block * kVariants[v].ppt;
+    const uint32_t chunk = kVariants[v].block * std::max(kVariants[v].ppt, 1u);
     std::vector<uint2> items;
     for (size_t s = 0; s < b->scen.size(); ++s)
         for (uint32_t l = 0; l < b->scen[s].capacity; l += chunk) items.push_back(make_uint2((uint32_t)s, l));

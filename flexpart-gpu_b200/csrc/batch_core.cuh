@@ -15,7 +15,7 @@
 namespace fpg {
 
 constexpr uint32_t TILE = 256;
-constexpr uint32_t kNumVariants = 8;   // compiled launch shapes of the particle pass
+constexpr uint32_t kNumVariants = 11;  // compiled launch shapes of the particle pass
 
 struct BatchState {
     int64_t t;

@@ -347,12 +347,14 @@ fpg_status fpg_batch_download_grids(fpg_batch* b, uint32_t* counts, uint32_t* ma
 /* Device-side error flags (1: a release fell outside the grid). */
 fpg_status fpg_batch_errors(fpg_batch* b, int32_t* flags);
 
-/* Launch shapes of the persistent particle pass (fpg_batch_tuning, fpg.h):
- * threads per CTA, CTAs resident per SM the kernel is compiled for (its
- * register budget), and particles per thread in one work item (a work item
- * is block_threads * particles_per_thread consecutive slots of one
- * scenario).  step_ms is the particle pass's time measured by the tuner (0
- * when set by hand).
+/* Launch shapes of the particle pass (fpg_batch_tuning, fpg.h): threads per
+ * CTA, CTAs resident per SM the kernel is compiled for (its register
+ * budget), and particles per thread in one work item (a work item is
+ * block_threads * particles_per_thread consecutive slots of one scenario),
+ * which persistent CTAs pull from a counter.  particles_per_thread 0 is the
+ * non-persistent pass: one CTA per item of block_threads slots, one slot per
+ * thread, launched over all items.  step_ms is the particle pass's time
+ * measured by the tuner (0 when set by hand).
  * The compiled launch shapes: writes up to max of them, returns their count. */
 uint32_t fpg_batch_tuning_candidates(fpg_batch_tuning* out, uint32_t max);
 /* Times the next step's particle pass under every compiled shape (best of
