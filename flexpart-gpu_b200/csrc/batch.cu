@@ -178,20 +178,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_step_flat_kernel(StepArgs a
         particle_step(a, global_levels(a), d.offset + local, local, st->alpha, d.counter, d.key0, d.key1);
 }
 
-// The launch shapes the particle pass is compiled for; the tuner picks one.
-// ppt 0: batch_step_flat_kernel, one CTA per item of `block` slots.
+// The launch shapes the particle pass is compiled for; the tuner picks one,
+// and the first is the default.  ppt 0: batch_step_flat_kernel, one CTA per
+// item of `block` slots.
 struct StepVariant {
     uint32_t block, minb, ppt;
     void (*kernel)(StepArgs, BatchState*, const ScenDev*, const uint2*, uint32_t);
 };
 
 const StepVariant kVariants[] = {
+    {128, 12, 0, batch_step_flat_kernel<128, 12>},
     {256, 4, 1, batch_step_kernel<256, 4, 1>}, {256, 4, 2, batch_step_kernel<256, 4, 2>},
     {256, 3, 1, batch_step_kernel<256, 3, 1>}, {256, 2, 1, batch_step_kernel<256, 2, 1>},
     {128, 8, 1, batch_step_kernel<128, 8, 1>}, {128, 8, 2, batch_step_kernel<128, 8, 2>},
     {512, 2, 1, batch_step_kernel<512, 2, 1>}, {256, 5, 1, batch_step_kernel<256, 5, 1>},
     {256, 5, 0, batch_step_flat_kernel<256, 5>}, {128, 10, 0, batch_step_flat_kernel<128, 10>},
-    {128, 12, 0, batch_step_flat_kernel<128, 12>},
 };
 static_assert(sizeof(kVariants) / sizeof(kVariants[0]) == kNumVariants, "launch shape table");
 
