@@ -120,10 +120,19 @@ class Batch:
     def particles(self) -> Particles:
         return _ParticlesView(self.ctx, lib.fpg_batch_particles(self.h))
 
-    def download_grids(self):
+    def download_grids(self, out=None):
+        """The per-scenario grids of the last output step as (counts, scaled
+        mass), u32 of shape (n_scenarios, nx, ny, nz); `out` may pass two
+        such C-contiguous arrays (page-locked ones copy fastest) to fill."""
         nx, ny, nz = self.out_shape
-        counts = np.zeros((self.n_scenarios, nx, ny, nz), np.uint32)
-        mass = np.zeros((self.n_scenarios, nx, ny, nz), np.uint32)
+        shape = (self.n_scenarios, nx, ny, nz)
+        if out is None:
+            counts, mass = np.zeros(shape, np.uint32), np.zeros(shape, np.uint32)
+        else:
+            counts, mass = out
+            for a in (counts, mass):
+                if a.shape != shape or a.dtype != np.uint32 or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"grid output arrays must be C-contiguous uint32 of shape {shape}")
         check(lib.fpg_batch_download_grids(self.h, _p(counts), _p(mass)), "fpg_batch_download_grids")
         return counts, mass
 
