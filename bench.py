@@ -1034,6 +1034,8 @@ def main():
                 pf[k] = torch.from_numpy(np.ascontiguousarray(f[k].reshape(-1))).pin_memory()
             pf["surface"] = torch.from_numpy(f["surface"].view(np.uint8)).pin_memory()
             pinned.append(pf)
+        precip_pinned = [torch.from_numpy(np.ascontiguousarray(p_, np.float32).reshape(-1)).pin_memory()
+                         for p_ in precip]
         drv.enable_met_ring(3)
         fs = spec.frame_seconds
         copy_stream = torch.cuda.Stream()
@@ -1053,7 +1055,7 @@ def main():
             prefetch(tb)
             if seen["bracket"] != (fa, fb, ta):
                 # the precipitation field of the bracket goes up with its wet forcing
-                wet_spin.from_precipitation(precip[fa], None, None, scn.wet_a, scn.wet_b)
+                wet_spin.from_precipitation(precip_pinned[fa].numpy(), None, None, scn.wet_a, scn.wet_b, sync=False)
                 h2d["bytes"] += precip[fa].nbytes
                 seen["bracket"] = (fa, fb, ta)
             drv.run_timestep(src.at(t), forcing)

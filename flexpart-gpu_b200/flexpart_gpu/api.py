@@ -283,11 +283,17 @@ class CellField:
         check(lib.fpg_cellfield_upload(self.h, _p(l_), _p(f_), None), "fpg_cellfield_upload")
         self.ctx.synchronize()
 
-    def from_precipitation(self, lsp, convp=None, cloud_cover=None, a: float = 1.0e-4, b: float = 0.8):
+    def from_precipitation(self, lsp, convp=None, cloud_cover=None, a: float = 1.0e-4, b: float = 0.8,
+                           sync: bool = True):
+        """Per-cell wet forcing from host precipitation fields.  With
+        sync=False the call returns once the work is queued: the arrays must
+        then stay alive and unchanged until the stream has run it (page-locked
+        arrays are copied asynchronously)."""
         arrs = [None if x is None else np.ascontiguousarray(x, np.float32).reshape(-1) for x in (lsp, convp, cloud_cover)]
         check(lib.fpg_cellfield_from_precipitation(self.h, *[None if x is None else _p(x) for x in arrs], a, b, None),
               "fpg_cellfield_from_precipitation")
-        self.ctx.synchronize()
+        if sync:
+            self.ctx.synchronize()
 
 
 def step(ctx: Context, particles: Particles, met: Met | None, pbl: Pbl | None, params: StepParams,
