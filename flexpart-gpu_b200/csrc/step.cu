@@ -383,7 +383,8 @@ extern "C" fpg_status fpg_pbl_diagnostics(fpg_ctx* ctx, const fpg_surface* surfa
     if (!surface->uploaded[0] || !surface->uploaded[1]) return FPG_ERR_NOT_READY;
     cudaStream_t s = ctx->pick(stream);
     const uint32_t n = (uint32_t)(pbl->nx * pbl->ny);
-    pbl_diag_kernel<<<blocks_for(n, 256), 256, 0, s>>>(surface->frame[0], surface->frame[1], alpha, *options, n,
+    // 64-thread CTAs spread the cells over more SMs (one cell per thread, a long dependent chain each)
+    pbl_diag_kernel<<<blocks_for(n, 64), 64, 0, s>>>(surface->frame[0], surface->frame[1], alpha, *options, n,
                                                         pbl->field[0], pbl->field[1], pbl->field[2], pbl->field[3],
                                                         pbl->field[4], pbl->field[5], pbl->field[6], pbl->packed,
                                                         pbl->hanna);
