@@ -184,20 +184,32 @@ __device__ __forceinline__ uint32_t source_level(float z, uint32_t L, const floa
     }
 }
 
+// The mixed height and the source level of one active slot.
+template <bool kSorted>
+__device__ __forceinline__ float mix_height(float z_in, uint32_t L, const float* __restrict__ iface,
+                                            const float* __restrict__ heights,
+                                            const uint32_t* __restrict__ has_weight, float z_min, float z_max,
+                                            int32_t& level_out) {
+    const float z = clampf(z_in, z_min, z_max);
+    const uint32_t level = source_level<kSorted>(z, L, iface);
+    level_out = (int32_t)level;
+    return __ldg(has_weight + level) ? __ldg(heights + level) : z;
+}
+
 template <bool kSorted>
 __device__ __forceinline__ void mix_slot(size_t p, float z_in, float* __restrict__ pos_z, int32_t* __restrict__ cbt,
                                          uint32_t L, const float* __restrict__ iface,
                                          const float* __restrict__ heights, const uint32_t* __restrict__ has_weight,
                                          float z_min, float z_max) {
-    const float z = clampf(z_in, z_min, z_max);
-    const uint32_t level = source_level<kSorted>(z, L, iface);
-    pos_z[p] = __ldg(has_weight + level) ? __ldg(heights + level) : z;
-    cbt[p] = (int32_t)level;
+    int32_t level;
+    pos_z[p] = mix_height<kSorted>(z_in, L, iface, heights, has_weight, z_min, z_max, level);
+    cbt[p] = level;
 }
 
 // Four slots per thread: the flags and heights of a quad arrive in one
-// 16-byte load each (the fields are 256-byte aligned); only active slots
-// are written.  The last n % 4 slots take scalar loads.
+// 16-byte load each (the fields are 256-byte aligned); a quad of active
+// slots is written with one 16-byte store per field, otherwise only the
+// active slots are written.  The last n % 4 slots take scalar loads.
 template <bool kSorted>
 __global__ void __launch_bounds__(256) conv_apply_kernel(size_t n, const uint32_t* __restrict__ flags,
                                                          float* __restrict__ pos_z, int32_t* __restrict__ cbt,
@@ -210,6 +222,17 @@ __global__ void __launch_bounds__(256) conv_apply_kernel(size_t n, const uint32_
     if (p0 + 4u <= n) {
         const uint4 f = __ldg(reinterpret_cast<const uint4*>(flags + p0));
         const float4 z = *reinterpret_cast<const float4*>(pos_z + p0);
+        if (f.x & f.y & f.z & f.w & FLAG_ACTIVE) {
+            int4 lv;
+            float4 zo;
+            zo.x = mix_height<kSorted>(z.x, L, iface, heights, has_weight, z_min, z_max, lv.x);
+            zo.y = mix_height<kSorted>(z.y, L, iface, heights, has_weight, z_min, z_max, lv.y);
+            zo.z = mix_height<kSorted>(z.z, L, iface, heights, has_weight, z_min, z_max, lv.z);
+            zo.w = mix_height<kSorted>(z.w, L, iface, heights, has_weight, z_min, z_max, lv.w);
+            *reinterpret_cast<float4*>(pos_z + p0) = zo;
+            *reinterpret_cast<int4*>(cbt + p0) = lv;
+            return;
+        }
         if (f.x & FLAG_ACTIVE) mix_slot<kSorted>(p0, z.x, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
         if (f.y & FLAG_ACTIVE) mix_slot<kSorted>(p0 + 1, z.y, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
         if (f.z & FLAG_ACTIVE) mix_slot<kSorted>(p0 + 2, z.z, pos_z, cbt, L, iface, heights, has_weight, z_min, z_max);
