@@ -119,11 +119,14 @@ __global__ void __launch_bounds__(256) cbl_sample_kernel(SlotView v, const fpg_h
 }
 
 // The fused form: sigma_w of compute_hanna at the slot's cell (the vertical
-// branch of hanna_short_w gives the same sigma_w bits as compute_hanna), and
-// the uniforms of one Philox block at counter + slot: u0, u1, u2 of
-// PhiloxRng::next_uniform4 on a stream that starts at that counter
-// (physics/cbl.rs:291-295, physics/rng.rs:130-164).
-__global__ void __launch_bounds__(256) cbl_sample_philox_kernel(SlotView v, const float4* __restrict__ pbl,
+// branch of hanna_short_w gives the same sigma_w bits as compute_hanna) from
+// the cell's Hanna constants (the floored u*, w*, h, the Obukhov length, the
+// regime and the constant products the PBL pass stores per cell, so the
+// per-cell part is not redone per slot), and the uniforms of one Philox
+// block at counter + slot: u0, u1, u2 of PhiloxRng::next_uniform4 on a
+// stream that starts at that counter (physics/cbl.rs:291-295,
+// physics/rng.rs:130-164).
+__global__ void __launch_bounds__(256) cbl_sample_philox_kernel(SlotView v, const CellHanna* __restrict__ hcell,
                                                                 uint32_t pnx, uint32_t pny, uint32_t k0,
                                                                 uint32_t k1, u32x4 counter,
                                                                 fpg_cbl_sampling_output* __restrict__ out) {
@@ -133,14 +136,12 @@ __global__ void __launch_bounds__(256) cbl_sample_philox_kernel(SlotView v, cons
         store_zero_output(out, p);
         return;
     }
-    const float4 cell = pbl_cell(v, p, pbl, pnx, pny);
-    const float ol = obukhov_from_inverse(cell.w);
+    const CellHanna cell = ld_cell_hanna(hcell + pbl_cell_index(v, p, pnx, pny));
     const float z = v.pos_z[p];
-    const float ust = fmaxf(cell.x, 1.0e-4f), wst = fmaxf(cell.y, 0.0f), h = fmaxf(cell.z, 1.0f);
     float sigw, dsigwdz, tlw;
-    hanna_short_w(ust, wst, ol, h, z, hanna_regime(ol, h), sigw, dsigwdz, tlw);
+    hanna_short_cell_t<float>(cell, z, sigw, dsigwdz, tlw);
     const u32x4 b = philox4x32_10(counter_add(counter, (uint32_t)p), k0, k1);
-    const CblPdf pdf = cbl_pdf(z, h, wst, sigw, ol);
+    const CblPdf pdf = cbl_pdf(z, cell.h, cell.wst, sigw, cell.ol);
     store_output(out, p, cbl_draw(pdf, u32_to_uniform01(b.x), u32_to_uniform01(b.y), u32_to_uniform01(b.z)), pdf);
 }
 
@@ -291,7 +292,7 @@ extern "C" fpg_status fpg_cbl_sample_philox(fpg_ctx* ctx, const fpg_particles* P
     if (!out_dev || !aligned16(out_dev)) return FPG_ERR_INVALID_ARGUMENT;
     const u32x4 c{counter[0], counter[1], counter[2], counter[3]};
     cbl_sample_philox_kernel<<<(unsigned)((v.n + 255) / 256), 256, 0, ctx->pick(stream)>>>(
-        v, pbl->packed, (uint32_t)pbl->nx, (uint32_t)pbl->ny, key[0], key[1], c, out_dev);
+        v, pbl->hanna, (uint32_t)pbl->nx, (uint32_t)pbl->ny, key[0], key[1], c, out_dev);
     ctx->count();
     FPG_CHECK_LAUNCH();
     return FPG_OK;

@@ -33,13 +33,17 @@ inline SlotView slot_view(const fpg_particles* P) {
 }
 
 // hanna_params.wgsl:244-250: the PBL cell of the particle's position.
-__device__ __forceinline__ float4 pbl_cell(const SlotView& v, size_t p, const float4* pbl, uint32_t pnx,
-                                           uint32_t pny) {
+__device__ __forceinline__ uint32_t pbl_cell_index(const SlotView& v, size_t p, uint32_t pnx, uint32_t pny) {
     const float x = (float)v.cell_x[p] + v.pos_x[p];
     const float y = (float)v.cell_y[p] + v.pos_y[p];
     const uint32_t i = (uint32_t)floorf(clampf(x, 0.0f, (float)(pnx - 1u)));
     const uint32_t j = (uint32_t)floorf(clampf(y, 0.0f, (float)(pny - 1u)));
-    return __ldg(pbl + (i * pny + j));
+    return i * pny + j;
+}
+
+__device__ __forceinline__ float4 pbl_cell(const SlotView& v, size_t p, const float4* pbl, uint32_t pnx,
+                                           uint32_t pny) {
+    return __ldg(pbl + pbl_cell_index(v, p, pnx, pny));
 }
 
 }  // namespace fpg
