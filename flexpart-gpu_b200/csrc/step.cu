@@ -744,8 +744,12 @@ struct RecordTurbArgs {
 
 // hanna_params.wgsl:231-258 with compute_hanna (physics/hanna.rs:49-163):
 // one 64-byte HannaParams record per slot, zeros for inactive slots.
-__global__ void __launch_bounds__(256) hanna_params_kernel(SlotView v, const float4* __restrict__ pbl, uint32_t pnx,
-                                                           uint32_t pny, fpg_hanna_params* __restrict__ out) {
+// compute_hanna at the slot's height from its cell's Hanna constants (the
+// record the PBL pass builds from the same u*, w*, h and 1/L, with the same
+// operations as compute_hanna would, so the results are the same bits).
+__global__ void __launch_bounds__(256) hanna_params_kernel(SlotView v, const CellHanna* __restrict__ hcell,
+                                                           uint32_t pnx, uint32_t pny,
+                                                           fpg_hanna_params* __restrict__ out) {
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= v.n) return;
     float4* o = reinterpret_cast<float4*>(out + p);
@@ -754,10 +758,9 @@ __global__ void __launch_bounds__(256) hanna_params_kernel(SlotView v, const flo
         o[0] = z; o[1] = z; o[2] = z; o[3] = z;
         return;
     }
-    const float4 cell = pbl_cell(v, p, pbl, pnx, pny);
-    const float ol = obukhov_from_inverse(cell.w);
+    const CellHanna cell = ld_cell_hanna(hcell + pbl_cell_index(v, p, pnx, pny));
     const float z = v.pos_z[p];
-    const Hanna hn = compute_hanna(cell.x, cell.y, ol, cell.z, z);
+    const Hanna hn = compute_hanna_cell_t<float>(cell, z);
     // zeta and d(sigma_w^2)/dz as the CPU routine forms them (hanna.rs:55,145)
     const float zeta = clampf(clampf(z, 0.0f, hn.h) / hn.h, 0.0f, 1.0f);
     o[0] = make_float4(hn.ust, hn.wst, hn.ol, hn.h);
@@ -854,7 +857,7 @@ extern "C" fpg_status fpg_dispatch_hanna_params(fpg_ctx* ctx, const fpg_particle
     const SlotView v = slot_view(P);
     if (v.n == 0) return FPG_OK;
     hanna_params_kernel<<<(unsigned)((v.n + 255) / 256), 256, 0, ctx->pick(stream)>>>(
-        v, pbl->packed, (uint32_t)pbl->nx, (uint32_t)pbl->ny, out_dev);
+        v, pbl->hanna, (uint32_t)pbl->nx, (uint32_t)pbl->ny, out_dev);
     ctx->count();
     FPG_CHECK_LAUNCH();
     return FPG_OK;
