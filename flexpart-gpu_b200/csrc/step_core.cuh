@@ -270,11 +270,21 @@ __device__ __forceinline__ void turbulence_from_hanna(const A& a, const CellHann
         tw = L::v(tw, sigw, tlw, dsigwdz, dt_sub, a.rho, eta);
         pz = pz + tw * dt_sub;
         if (h > zmin) {
+            // the first bounce by selects (most sub-steps need none or one, and
+            // a warp's lanes disagree on which), the loop only for the rest
             T z = pz;
-            for (int bounce = 0; bounce < 10; ++bounce) {
-                if (val(z) < zmin) { z = 2.0f * zmin - z; cbt = -cbt; tw = -tw; }
-                else if (val(z) > h) { z = 2.0f * h - z; cbt = -cbt; tw = -tw; }
-                else break;
+            const bool lo = val(z) < zmin, hi = !lo && val(z) > h;
+            const bool any = lo || hi;
+            const T zr = lo ? T(2.0f * zmin - z) : T(2.0f * h - z);
+            z = any ? zr : z;
+            cbt = any ? -cbt : cbt;
+            tw = any ? T(-tw) : tw;
+            if (any && (val(z) < zmin || val(z) > h)) {
+                for (int bounce = 1; bounce < 10; ++bounce) {
+                    if (val(z) < zmin) { z = 2.0f * zmin - z; cbt = -cbt; tw = -tw; }
+                    else if (val(z) > h) { z = 2.0f * h - z; cbt = -cbt; tw = -tw; }
+                    else break;
+                }
             }
             pz = xclamp(z, zmin, h);
         }
