@@ -61,20 +61,20 @@ ADJOINT_HBM_BUDGET = 140e9  # device bytes the batched adjoint may hold (the 150
 # 24 / 32 / 48 / 96 steps gives 1.297 / 1.318 / 1.324 / 1.335e10
 # particle-steps/s.  A reorder costs about 0.94 ms and the step kernel gains
 # little from it beyond the first step after it (the turbulence mixes the
-# heights within each column at once: 0.593 ms right after a reorder, 0.63
+# heights within each column at once: 0.582 ms right after a reorder, 0.618
 # ms from the second step on).  The default window of timed steps is one
 # reorder period, and its first step reorders.
 SORT_EVERY = 96
 # DRAM bytes (read + write) per particle of one fused-step launch, from an
 # ncu capture of a 10 M-particle launch of the global run's population
 # (bench.py --quick: particles around the 8 sources, reordered by met cell
-# before the timed steps): 443.2 MB read + 422.1 MB written = 86.5 B per
+# before the timed steps): 443.2 MB read + 421.9 MB written = 86.5 B per
 # particle against the algorithmic 96 B (44 B read, 52 B written); the last
 # ~100 MB of writes are still in the 126 MB L2 when the kernel ends.
-DRAM_BYTES_PER_PARTICLE_NCU = (443.2e6 + 422.1e6) / 10.0e6
+DRAM_BYTES_PER_PARTICLE_NCU = (443.2e6 + 421.9e6) / 10.0e6
 # Warp instructions per 32 particle-steps (smsp__inst_executed.sum of the
-# same capture: 560.9 M for 10 M particles).
-WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 560.9e6 / (10.0e6 / 32)
+# same capture: 553.5 M for 10 M particles).
+WARP_INSTRUCTIONS_PER_32_PARTICLES_NCU = 553.5e6 / (10.0e6 / 32)
 
 
 def issue_roofline(n_particles, kernel_ms, clk):
